@@ -1,0 +1,142 @@
+/*
+ * tlibttm.h — C ABI of the B200 mode-q tensor-times-matrix library
+ * (libtlibttm_cuda.so).
+ *
+ * This is the boundary a foreign caller (C, ctypes/cffi, cgo, JNI, the C++
+ * header include/tlib/ttm.h) binds. Signatures use only plain pointers,
+ * size_t metadata arrays and an opaque CUDA stream; no C++ or torch types.
+ *
+ * Semantics follow the reference tlib::ttm (bassoy/ttm):
+ *   C(i1..j..ip) = sum_{iq} A(i1..iq..ip) * B(j,iq)     (README.md:13-18)
+ * with C overwritten (beta = 0, include/tlib/detail/mtm.h:92), C laid out with
+ * A's layout pi, B of shape nb = (m, n_q) column-major when pib[0] == 1 and
+ * row-major otherwise (include/tlib/detail/ttm.h:417), all metadata one-based
+ * as in the reference, and the reference's argument checks with the same
+ * message texts (include/tlib/ttm.h:65-90).
+ *
+ * Pointers: a, b and c may each be host memory or device memory of the
+ * current CUDA device (managed memory counts as device memory). The library
+ * detects which with cudaPointerGetAttributes. If any of them is host memory,
+ * it is staged through device buffers the library owns and the call blocks
+ * until the result is back in host memory. If all three are device memory,
+ * the work is enqueued on `stream` (NULL = the legacy default stream) and the
+ * call returns without waiting. The metadata arrays (na, wa, ... ) are always
+ * host memory and are not retained after the call.
+ *
+ * Return value: TLIBTTM_OK (0) or one of the error codes below; the text of
+ * the last error on the calling thread is returned by tlibttm_last_error().
+ */
+#ifndef TLIBTTM_H
+#define TLIBTTM_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum tlibttm_status {
+    TLIBTTM_OK = 0,
+    TLIBTTM_ERR_ARG = 1,         /* argument check failed (text = reference runtime_error text) */
+    TLIBTTM_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    TLIBTTM_ERR_ALLOC = 3,       /* device or pinned-host allocation failed */
+    TLIBTTM_ERR_UNSUPPORTED = 4, /* valid arguments that this build cannot run (e.g. dtype/precision pair) */
+    TLIBTTM_ERR_DEVICE = 5       /* a kernel reported failure through its device status word */
+};
+
+enum tlibttm_dtype {
+    TLIBTTM_F32 = 0,
+    TLIBTTM_F64 = 1
+};
+
+/*
+ * Arithmetic used for the contraction.
+ *  PLAIN   exact IEEE FMA in the I/O type (FP32 FFMA / FP64 DFMA). Default.
+ *  BF16X3  float only: each FP32 operand is split into bf16 hi + lo parts and
+ *          hi*hi + hi*lo + lo*hi run on the tcgen05 tensor cores with FP32
+ *          accumulation in TMEM.
+ *  FP8     float only: e4m3 operands with a power-of-two scale per slice
+ *          (per fibre of A and per row of B), FP32 accumulation. Approximate.
+ *  OZAKI   double only: FP64 operands split into int8 slices with a shared
+ *          power-of-two exponent per fibre, exact int32 tensor-core products,
+ *          FP64 recombination.
+ *  AUTO    the library picks per problem (tuned choice among the exact and
+ *          the FP32-accurate paths; never FP8).
+ * Small-m problems (bandwidth-bound) always run the PLAIN bandwidth kernels.
+ */
+enum tlibttm_precision {
+    TLIBTTM_PREC_DEFAULT = 0,
+    TLIBTTM_PREC_PLAIN = 1,
+    TLIBTTM_PREC_BF16X3 = 2,
+    TLIBTTM_PREC_FP8 = 3,
+    TLIBTTM_PREC_OZAKI = 4,
+    TLIBTTM_PREC_AUTO = 5
+};
+
+/*
+ * Replaces tlib::ttm::ttm<float>(ep,sp,fp, q,p, a,na,wa,pia, b,nb,pib, c,nc,wc)
+ * (reference include/tlib/ttm.h:54-93). The three policy tags select CPU
+ * threading in the reference and have no counterpart on the GPU, so they are
+ * not part of the ABI. Uses the process-wide default precision
+ * (tlibttm_set_precision, initially PLAIN).
+ */
+int tlibttm_ttm_f32(unsigned q, unsigned p,
+                    const float* a, const size_t* na, const size_t* wa, const size_t* pia,
+                    const float* b, const size_t* nb, const size_t* pib,
+                    float* c, const size_t* nc, const size_t* wc,
+                    void* stream);
+
+/* Same as tlibttm_ttm_f32 for double (reference include/tlib/ttm.h:54-93 with value_t = double). */
+int tlibttm_ttm_f64(unsigned q, unsigned p,
+                    const double* a, const size_t* na, const size_t* wa, const size_t* pia,
+                    const double* b, const size_t* nb, const size_t* pib,
+                    double* c, const size_t* nc, const size_t* wc,
+                    void* stream);
+
+/*
+ * Explicit-precision form of the two calls above (an extension: the
+ * reference has one arithmetic, its BLAS's). dtype is a tlibttm_dtype,
+ * precision a tlibttm_precision.
+ */
+int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p,
+                   const void* a, const size_t* na, const size_t* wa, const size_t* pia,
+                   const void* b, const size_t* nb, const size_t* pib,
+                   void* c, const size_t* nc, const size_t* wc,
+                   void* stream);
+
+/* Text of the last error reported on the calling thread ("" if none). */
+const char* tlibttm_last_error(void);
+
+/* Process-wide default precision used by tlibttm_ttm_f32/_f64. Returns the previous value. */
+int tlibttm_set_precision(int precision);
+int tlibttm_get_precision(void);
+
+/* Name of the kernel the last successful call on this thread launched (diagnostics, tests). */
+const char* tlibttm_last_kernel(void);
+
+/* Number of kernels this library launched on the calling thread since the last reset. */
+unsigned long long tlibttm_launch_count(int reset);
+
+/* Waits for all work the library enqueued on `stream`. */
+int tlibttm_synchronize(void* stream);
+
+/* Releases the library's staging buffers on the current device. */
+int tlibttm_release_buffers(void);
+
+/*
+ * Layout / stride helpers with the reference's semantics, for callers that
+ * build metadata without the C++ header:
+ *   tlibttm_k_order_layout  reference include/tlib/detail/layout.h:57-76
+ *   tlibttm_inverse_mode    reference include/tlib/detail/layout.h:120-144 (0 on error)
+ *   tlibttm_strides         reference include/tlib/detail/strides.h:31-57 (incl. the
+ *                           all-ones strides of vector/scalar shapes)
+ */
+int tlibttm_k_order_layout(size_t* layout, size_t p, size_t k);
+size_t tlibttm_inverse_mode(const size_t* layout, size_t p, size_t mode);
+int tlibttm_strides(const size_t* shape, size_t p, const size_t* layout, size_t* strides);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TLIBTTM_H */

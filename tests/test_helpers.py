@@ -1,0 +1,128 @@
+"""Layout / shape / stride helpers and the C++ drop-in headers, against the
+reference's own tables (test/src/gtest_tlib_{layout,strides,shape}.cpp) and,
+when present, the reference build itself."""
+import itertools
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from ttm_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_ROOT = "/root/reference"
+
+
+def test_k_order_layouts_table():
+    # gtest_tlib_layout.cpp:40-166: k-order layouts of orders 1..4 for k = 1..4.
+    want = {1: [[1], [1, 2], [1, 2, 3], [1, 2, 3, 4]],
+            2: [[1], [2, 1], [2, 1, 3], [2, 1, 3, 4]],
+            3: [[1], [2, 1], [3, 2, 1], [3, 2, 1, 4]],
+            4: [[1], [2, 1], [3, 2, 1], [4, 3, 2, 1]]}
+    for k, rows in want.items():
+        for p, row in enumerate(rows, start=1):
+            assert _lib.k_order_layout(p, k) == row
+    assert _lib.k_order_layout(4, 0) == [4, 3, 2, 1]
+
+
+def test_inverse_mode_all_k_orders():
+    # gtest_tlib_layout.cpp:191-211
+    for order in range(1, 11):
+        for k in range(1, order + 1):
+            lay = _lib.k_order_layout(order, k)
+            for mode in range(1, order + 1):
+                r = _lib.inverse_mode(lay, mode)
+                assert 1 <= r <= order and lay[r - 1] == mode
+    with pytest.raises(RuntimeError, match="mode should be one-based"):
+        _lib.inverse_mode([1, 2], 3)
+    with pytest.raises(RuntimeError, match="input layout is not valid"):
+        _lib.inverse_mode([1, 1], 1)
+
+
+def test_strides_tables():
+    # gtest_tlib_strides.cpp:34-147
+    assert _lib.strides([1], [1]) == [1]
+    assert _lib.strides([1, 1], [1, 2]) == [1, 1]
+    for ext in ([1, 2], [1, 4], [1, 8], [2, 1], [4, 1], [8, 1]):
+        for lay in ([1, 2], [2, 1]):
+            assert _lib.strides(ext, lay) == [1, 1]
+    for ext in ([2, 2], [2, 4], [4, 2], [4, 4], [2, 8], [8, 2], [4, 8], [8, 4], [8, 8]):
+        assert _lib.strides(ext, [1, 2]) == [1, ext[0]]
+        assert _lib.strides(ext, [2, 1]) == [ext[1], 1]
+    first = ([2, 1, 2], [1, 2, 2]), ([1, 2, 2], [1, 1, 2]), ([2, 2, 2], [1, 2, 4]), ([2, 4, 2], [1, 2, 8]), \
+            ([4, 4, 2], [1, 4, 16]), ([2, 4, 4], [1, 2, 8])
+    for ext, ref in first:
+        assert _lib.strides(ext, [1, 2, 3]) == ref
+    last = ([2, 1, 2], [2, 2, 1]), ([1, 2, 2], [4, 2, 1]), ([2, 2, 2], [4, 2, 1]), ([2, 4, 2], [8, 2, 1]), \
+           ([2, 4, 4], [16, 4, 1])
+    for ext, ref in last:
+        assert _lib.strides(ext, [3, 2, 1]) == ref
+    second = ([2, 1, 2], [1, 1, 2]), ([1, 2, 2], [2, 1, 2]), ([2, 2, 2], [2, 1, 4]), ([2, 4, 2], [4, 1, 8]), \
+             ([2, 2, 4], [2, 1, 4]), ([4, 2, 2], [2, 1, 8])
+    for ext, ref in second:
+        assert _lib.strides(ext, [2, 1, 3]) == ref
+
+
+def test_helpers_match_reference_build(reference):
+    for p in range(1, 6):
+        for k in range(0, p + 1):
+            assert _lib.k_order_layout(p, k) == reference.k_order_layout(p, k)
+        for n in itertools.product([1, 2, 3], repeat=p):
+            for pi in itertools.permutations(range(1, p + 1)):
+                assert _lib.strides(list(n), list(pi)) == reference.strides(list(n), list(pi)), (n, pi)
+
+
+CXX_PROBE = r"""
+#include <tlib/ttm.h>
+#include <cassert>
+#include <vector>
+using namespace tlib::ttm;
+int main() {
+    // shape / layout / strides predicates, gtest_tlib_shape.cpp:65-139
+    std::vector<std::vector<unsigned>> s = {{}, {0}, {1}, {2}, {0,1}, {1,0}, {1,1}, {2,1}, {3,1}, {1,2}, {1,3},
+        {2,2}, {3,3}, {0,1,1}, {1,1,0}, {1,1,1}, {1,1,2}, {1,2,1}, {1,2,2}, {2,1,1}, {2,1,2}, {2,2,1}, {2,2,2}};
+    std::vector<int> scal = {2,6,15}, vec = {3,7,8,9,10,17,19}, mat = {11,12,21}, ten = {16,18,20,22}, inv = {0,1,4,5,13,14};
+    auto in = [](std::vector<int> const& v, int i){ for (int x : v) if (x == i) return true; return false; };
+    for (int i = 0; i < (int)s.size(); ++i) {
+        auto b = s[i].begin(), e = s[i].end();
+        if (detail::is_scalar(b,e) != in(scal,i)) return 10 + i;
+        if (detail::is_vector(b,e) != in(vec,i)) return 40 + i;
+        if (detail::is_matrix(b,e) != in(mat,i)) return 70 + i;
+        if (detail::is_tensor(b,e) != in(ten,i)) return 100 + i;
+        if (detail::is_valid_shape(b,e) == in(inv,i)) return 130 + i;
+    }
+    std::vector<std::vector<unsigned>> bad = {{}, {0}, {0,1}, {1,0}, {0,2}, {2,0}, {2,1,0}, {3,0,2}, {3,1,4}, {1,3,4}, {1,3,5}};
+    for (auto const& l : bad) if (detail::is_valid_layout(l.begin(), l.end())) return 160;
+    std::size_t pi3[3] = {2,1,3};
+    if (!detail::is_case<8>(3u, 1, pi3) || detail::is_case<6>(3u, 1, pi3) || !detail::is_case<6>(3u, 2, pi3)) return 170;
+    auto A = tensor<float>({4,3,2});
+    if (A.strides() != std::vector<std::size_t>({1,4,12})) return 180;
+    try { A(4); return 190; } catch (std::runtime_error const&) {}
+    return 0;
+}
+"""
+
+
+def test_cpp_headers_compile_and_predicates(tmp_path):
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("g++ not available")
+    src = tmp_path / "probe.cpp"
+    src.write_text(CXX_PROBE)
+    exe = tmp_path / "probe"
+    subprocess.run([gxx, "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", os.path.join(ROOT, "ttm_b200"), "-ltlibttm_cuda",
+                    "-Wl,-rpath," + os.path.join(ROOT, "ttm_b200")], check=True)
+    r = subprocess.run([str(exe)])
+    assert r.returncode == 0, r.returncode
+
+
+@pytest.mark.parametrize("name", ["interface1", "interface2", "interface3", "measure"])
+def test_reference_examples_compile_unchanged(tmp_path, name):
+    """The reference's own example programs build against include/ without edits."""
+    src = os.path.join(REF_ROOT, "example", name + ".cpp")
+    if not os.path.exists(src):
+        pytest.skip("reference sources not present")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-c", src, "-o",
+                    str(tmp_path / (name + ".o"))], check=True)

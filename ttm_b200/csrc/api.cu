@@ -1,0 +1,436 @@
+// C ABI of the B200 TTM library: argument checks, device planner, staging of
+// host operands, kernel dispatch. Declarations and contract: include/tlibttm.h.
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "tlibttm.h"
+#include "tlib/detail/layout.h"
+#include "tlib/detail/shape.h"
+#include "tlib/detail/strides.h"
+
+#include "common.cuh"
+#include "tc_kernels.cuh"
+
+namespace tlibttm {
+
+const char* kernel_name(int id)
+{
+    switch (id) {
+    case K_SIMT_GEMM: return "simt_gemm";
+    case K_COLVEC: return "colvec";
+    case K_ROWDOT: return "rowdot";
+    case K_STRIDED: return "strided";
+    case K_TC_BF16X3: return "tc_bf16x3";
+    case K_TC_FP8: return "tc_fp8";
+    case K_TC_OZAKI: return "tc_ozaki";
+    case K_SPLIT_B: return "split_b";
+    default: return "";
+    }
+}
+
+namespace {
+
+thread_local std::string g_err;
+thread_local const char* g_last_kernel = "";
+thread_local unsigned long long g_launches = 0;
+
+int initial_precision()
+{
+    const char* e = std::getenv("TLIBTTM_PRECISION");
+    if (!e) return TLIBTTM_PREC_PLAIN;
+    if (!std::strcmp(e, "plain")) return TLIBTTM_PREC_PLAIN;
+    if (!std::strcmp(e, "bf16x3")) return TLIBTTM_PREC_BF16X3;
+    if (!std::strcmp(e, "fp8")) return TLIBTTM_PREC_FP8;
+    if (!std::strcmp(e, "ozaki")) return TLIBTTM_PREC_OZAKI;
+    if (!std::strcmp(e, "auto")) return TLIBTTM_PREC_AUTO;
+    return TLIBTTM_PREC_PLAIN;
+}
+
+std::atomic<int> g_precision{initial_precision()};
+
+int fail(int code, const std::string& msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+    g_err = std::string("tlibttm: CUDA error in ") + where + ": " + cudaGetErrorString(e);
+    return TLIBTTM_ERR_CUDA;
+}
+
+struct Args {
+    int dtype;
+    unsigned q, p;
+    const void* a;
+    const size_t *na, *wa, *pia;
+    const void* b;
+    const size_t *nb, *pib;
+    void* c;
+    const size_t *nc, *wc;
+};
+
+// Reference include/tlib/ttm.h:65-90: same checks, same order, same texts.
+// Two additions the reference leaves to asserts or crashes: a null pib, and
+// C extents that differ from A's outside mode q (include/tlib/detail/mtm.h:166-167).
+int validate(const Args& x)
+{
+    static const std::string E = "Error in tlib::tensor_times_matrix: ";
+    if (x.p == 0) return fail(TLIBTTM_ERR_ARG, E + "input tensor order should be greater zero.");
+    if (x.q == 0 || x.q > x.p) return fail(TLIBTTM_ERR_ARG, E + "contraction mode should be greater zero or less than or equal to p.");
+    if (!x.a) return fail(TLIBTTM_ERR_ARG, E + "pointer to input tensor A should not be zero.");
+    if (!x.b) return fail(TLIBTTM_ERR_ARG, E + "pointer to input vector B should not be zero.");
+    if (!x.c) return fail(TLIBTTM_ERR_ARG, E + "pointer to output tensor C should not be zero.");
+    if (!x.na) return fail(TLIBTTM_ERR_ARG, E + "pointer to input tensor shape vector na should not be zero.");
+    if (!x.nb) return fail(TLIBTTM_ERR_ARG, E + "pointer to input vector shape vector nb should not be zero.");
+    if (!x.nc) return fail(TLIBTTM_ERR_ARG, E + "pointer to output tensor shape vector nc should not be zero.");
+    if (!x.wa) return fail(TLIBTTM_ERR_ARG, E + "pointer to input tensor stride vector wa should not be zero.");
+    if (!x.wc) return fail(TLIBTTM_ERR_ARG, E + "pointer to output tensor stride vector wc should not be zero.");
+    if (!x.pia) return fail(TLIBTTM_ERR_ARG, E + "pointer to input tensor permutation vector pia should not be zero.");
+    if (x.na[x.q - 1] != x.nb[1]) return fail(TLIBTTM_ERR_ARG, E + "contraction dimension of A and B are not equal.");
+    if (x.nc[x.q - 1] != x.nb[0]) return fail(TLIBTTM_ERR_ARG, E + "free dimension of C and B are not equal.");
+    if (!tlib::ttm::detail::is_valid_shape(x.na, x.na + x.p)) return fail(TLIBTTM_ERR_ARG, E + "shape vector of A is not valid.");
+    if (!tlib::ttm::detail::is_valid_shape(x.nc, x.nc + x.p)) return fail(TLIBTTM_ERR_ARG, E + "shape vector of C is not valid.");
+    if (!tlib::ttm::detail::is_valid_layout(x.pia, x.pia + x.p)) return fail(TLIBTTM_ERR_ARG, E + "layout vector of A is not valid.");
+    if (!tlib::ttm::detail::is_valid_strides(x.pia, x.pia + x.p, x.wa)) return fail(TLIBTTM_ERR_ARG, E + "stride vector of A is not valid.");
+    if (!tlib::ttm::detail::is_valid_strides(x.pia, x.pia + x.p, x.wc)) return fail(TLIBTTM_ERR_ARG, E + "stride vector of C is not valid.");
+    if (!x.pib) return fail(TLIBTTM_ERR_ARG, E + "pointer to input matrix layout vector pib should not be zero.");
+    for (unsigned r = 0; r < x.p; ++r)
+        if (r != x.q - 1 && x.nc[r] != x.na[r])
+            return fail(TLIBTTM_ERR_ARG, E + "shape vector of C does not match A outside the contraction mode.");
+    return TLIBTTM_OK;
+}
+
+// True iff strides w are the dense strides of extents n under layout pi,
+// ignoring modes of extent 1 (whose stride never enters an address).
+bool dense_under(const size_t* n, const size_t* w, const size_t* pi, unsigned p)
+{
+    size_t expect = 1;
+    for (unsigned r = 0; r < p; ++r) {
+        const size_t mode = pi[r] - 1;
+        if (n[mode] == 1) continue;
+        if (w[mode] != expect) return false;
+        expect *= n[mode];
+    }
+    return true;
+}
+
+size_t span_of(const size_t* n, const size_t* w, unsigned p)
+{
+    size_t s = 1;
+    for (unsigned r = 0; r < p; ++r) s += (n[r] - 1) * w[r];
+    return s;
+}
+
+struct Plan {
+    bool dense = true;
+    View3 v{};
+    StridedProblem sp{};
+    size_t a_elems = 0, b_elems = 0, c_elems = 0;   // element spans to stage
+};
+
+int make_plan(const Args& x, Plan& pl)
+{
+    const unsigned p = x.p, q = x.q;
+    const size_t* pia = x.pia;
+    unsigned qh = 0;
+    while (pia[qh] != q) ++qh;   // zero-based position of q in the layout
+    int64_t inner = 1, outer = 1;
+    for (unsigned r = 0; r < qh; ++r) inner *= (int64_t)x.na[pia[r] - 1];
+    for (unsigned r = qh + 1; r < p; ++r) outer *= (int64_t)x.na[pia[r] - 1];
+    const int64_t nq = (int64_t)x.na[q - 1], m = (int64_t)x.nb[0];
+
+    pl.dense = dense_under(x.na, x.wa, pia, p) && dense_under(x.nc, x.wc, pia, p);
+    pl.b_elems = (size_t)(m * nq);
+    if (pl.dense) {
+        pl.a_elems = (size_t)(outer * nq * inner);
+        pl.c_elems = (size_t)(outer * m * inner);
+        pl.v.outer = outer;
+        pl.v.nq = nq;
+        pl.v.inner = inner;
+        pl.v.m = m;
+        pl.v.b_cm = x.pib[0] == 1;
+    } else {
+        if (p > (unsigned)kMaxOrder)
+            return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm: non-dense strides are supported up to order 32.");
+        pl.a_elems = span_of(x.na, x.wa, p);
+        pl.c_elems = span_of(x.nc, x.wc, p);
+        StridedProblem& sp = pl.sp;
+        sp.p = (int)p;
+        sp.q = (int)q - 1;
+        sp.b_cm = x.pib[0] == 1;
+        sp.nq = nq;
+        sp.m = m;
+        sp.total = 1;
+        for (unsigned r = 0; r < p; ++r) {
+            sp.order[r] = (int)pia[r] - 1;
+            sp.nc[r] = (int64_t)x.nc[r];
+            sp.wa[r] = (int64_t)x.wa[r];
+            sp.wc[r] = (int64_t)x.wc[r];
+            sp.total *= (int64_t)x.nc[r];
+        }
+    }
+    return TLIBTTM_OK;
+}
+
+int note_launch(cudaError_t e, int kid)
+{
+    if (e != cudaSuccess) return cuda_fail(e, kernel_name(kid));
+    g_last_kernel = kernel_name(kid);
+    ++g_launches;
+    return TLIBTTM_OK;
+}
+
+// All operands are device memory: enqueue on stream s.
+int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
+{
+    if (!pl.dense) {
+        pl.sp.a = x.a;
+        pl.sp.b = x.b;
+        pl.sp.c = x.c;
+        return note_launch(launch_strided(pl.sp, x.dtype, s), K_STRIDED);
+    }
+    View3& v = pl.v;
+    v.a = x.a;
+    v.b = x.b;
+    v.c = x.c;
+    if (v.m <= kSmallM) {
+        if (v.inner == 1) return note_launch(launch_rowdot(v, x.dtype, s), K_ROWDOT);
+        return note_launch(launch_colvec(v, x.dtype, s), K_COLVEC);
+    }
+    if (precision == TLIBTTM_PREC_DEFAULT) precision = g_precision.load();
+    if (precision == TLIBTTM_PREC_AUTO)
+        precision = (x.dtype == TLIBTTM_F32 && tc_supported(v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3
+                                                                                     : TLIBTTM_PREC_PLAIN;
+    if (precision == TLIBTTM_PREC_BF16X3 || precision == TLIBTTM_PREC_FP8) {
+        if (x.dtype != TLIBTTM_F32)
+            return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm: the bf16x3 and fp8 precisions take float operands.");
+    }
+    if (precision == TLIBTTM_PREC_OZAKI && x.dtype != TLIBTTM_F64)
+        return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm: the ozaki precision takes double operands.");
+    if (precision != TLIBTTM_PREC_PLAIN && tc_supported(v, precision)) {
+        int kid = K_NONE;
+        cudaError_t e = launch_tc(v, precision, s, &kid);
+        return note_launch(e, kid);
+    }
+    return note_launch(launch_simt_gemm(v, x.dtype, s), K_SIMT_GEMM);
+}
+
+// ---- staging of host operands ---------------------------------------------------------------
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct Pool {
+    std::mutex mu;
+    DevBuf a, b, c;
+};
+
+std::mutex g_pools_mu;
+std::unordered_map<int, Pool*> g_pools;
+
+Pool& pool_for(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_pools_mu);
+    Pool*& p = g_pools[dev];
+    if (!p) p = new Pool();
+    return *p;
+}
+
+cudaError_t ensure(DevBuf& b, size_t bytes)
+{
+    if (b.bytes >= bytes) return cudaSuccess;
+    if (b.ptr) {
+        cudaError_t e = cudaFree(b.ptr);
+        b.ptr = nullptr;
+        b.bytes = 0;
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    if (e == cudaSuccess) b.bytes = bytes;
+    return e;
+}
+
+enum class Where { Host, Device };
+
+int classify(const void* ptr, int dev, Where& w)
+{
+    cudaPointerAttributes at;
+    cudaError_t e = cudaPointerGetAttributes(&at, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        w = Where::Host;
+        return TLIBTTM_OK;
+    }
+    if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) {
+        if (at.type == cudaMemoryTypeDevice && at.device != dev)
+            return fail(TLIBTTM_ERR_ARG, "tlibttm: device operand lives on a device other than the current one.");
+        w = Where::Device;
+    } else {
+        w = Where::Host;
+    }
+    return TLIBTTM_OK;
+}
+
+int run(const Args& x, int precision, void* stream)
+{
+    int rc = validate(x);
+    if (rc) return rc;
+    Plan pl;
+    rc = make_plan(x, pl);
+    if (rc) return rc;
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    Where wa, wb, wc;
+    if ((rc = classify(x.a, dev, wa)) || (rc = classify(x.b, dev, wb)) || (rc = classify(x.c, dev, wc))) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    if (wa == Where::Device && wb == Where::Device && wc == Where::Device) return run_device(x, pl, precision, s);
+
+    // At least one host operand: stage through the pool and block until done.
+    const size_t es = x.dtype == TLIBTTM_F32 ? sizeof(float) : sizeof(double);
+    Pool& pool = pool_for(dev);
+    std::lock_guard<std::mutex> lk(pool.mu);
+    Args d = x;
+    if (wa == Where::Host) {
+        if ((e = ensure(pool.a, pl.a_elems * es)) != cudaSuccess) return fail(TLIBTTM_ERR_ALLOC, "tlibttm: staging allocation for A failed.");
+        if ((e = cudaMemcpyAsync(pool.a.ptr, x.a, pl.a_elems * es, cudaMemcpyHostToDevice, s)) != cudaSuccess) return cuda_fail(e, "copy of A");
+        d.a = pool.a.ptr;
+    }
+    if (wb == Where::Host) {
+        if ((e = ensure(pool.b, pl.b_elems * es)) != cudaSuccess) return fail(TLIBTTM_ERR_ALLOC, "tlibttm: staging allocation for B failed.");
+        if ((e = cudaMemcpyAsync(pool.b.ptr, x.b, pl.b_elems * es, cudaMemcpyHostToDevice, s)) != cudaSuccess) return cuda_fail(e, "copy of B");
+        d.b = pool.b.ptr;
+    }
+    if (wc == Where::Host) {
+        if ((e = ensure(pool.c, pl.c_elems * es)) != cudaSuccess) return fail(TLIBTTM_ERR_ALLOC, "tlibttm: staging allocation for C failed.");
+        // A non-dense C has gaps the kernel does not write: bring them along so they survive.
+        if (!pl.dense)
+            if ((e = cudaMemcpyAsync(pool.c.ptr, x.c, pl.c_elems * es, cudaMemcpyHostToDevice, s)) != cudaSuccess) return cuda_fail(e, "copy of C");
+        d.c = pool.c.ptr;
+    }
+    rc = run_device(d, pl, precision, s);
+    if (rc) {
+        cudaStreamSynchronize(s);
+        return rc;
+    }
+    if (wc == Where::Host)
+        if ((e = cudaMemcpyAsync(x.c, d.c, pl.c_elems * es, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "copy of C");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    return TLIBTTM_OK;
+}
+
+}  // namespace
+}  // namespace tlibttm
+
+using namespace tlibttm;
+
+extern "C" {
+
+int tlibttm_ttm_f32(unsigned q, unsigned p, const float* a, const size_t* na, const size_t* wa,
+                    const size_t* pia, const float* b, const size_t* nb, const size_t* pib, float* c,
+                    const size_t* nc, const size_t* wc, void* stream)
+{
+    Args x{TLIBTTM_F32, q, p, a, na, wa, pia, b, nb, pib, c, nc, wc};
+    return run(x, TLIBTTM_PREC_DEFAULT, stream);
+}
+
+int tlibttm_ttm_f64(unsigned q, unsigned p, const double* a, const size_t* na, const size_t* wa,
+                    const size_t* pia, const double* b, const size_t* nb, const size_t* pib, double* c,
+                    const size_t* nc, const size_t* wc, void* stream)
+{
+    Args x{TLIBTTM_F64, q, p, a, na, wa, pia, b, nb, pib, c, nc, wc};
+    return run(x, TLIBTTM_PREC_DEFAULT, stream);
+}
+
+int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p, const void* a, const size_t* na,
+                   const size_t* wa, const size_t* pia, const void* b, const size_t* nb, const size_t* pib,
+                   void* c, const size_t* nc, const size_t* wc, void* stream)
+{
+    if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
+    if (precision < TLIBTTM_PREC_DEFAULT || precision > TLIBTTM_PREC_AUTO)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown precision.");
+    Args x{dtype, q, p, a, na, wa, pia, b, nb, pib, c, nc, wc};
+    return run(x, precision, stream);
+}
+
+const char* tlibttm_last_error(void) { return g_err.c_str(); }
+
+int tlibttm_set_precision(int precision)
+{
+    if (precision < TLIBTTM_PREC_PLAIN || precision > TLIBTTM_PREC_AUTO) return -1;
+    return g_precision.exchange(precision);
+}
+
+int tlibttm_get_precision(void) { return g_precision.load(); }
+
+const char* tlibttm_last_kernel(void) { return g_last_kernel; }
+
+unsigned long long tlibttm_launch_count(int reset)
+{
+    unsigned long long n = g_launches;
+    if (reset) g_launches = 0;
+    return n;
+}
+
+int tlibttm_synchronize(void* stream)
+{
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? TLIBTTM_OK : cuda_fail(e, "cudaStreamSynchronize");
+}
+
+int tlibttm_release_buffers(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return TLIBTTM_ERR_CUDA;
+    Pool& pool = pool_for(dev);
+    std::lock_guard<std::mutex> lk(pool.mu);
+    for (DevBuf* b : {&pool.a, &pool.b, &pool.c}) {
+        if (b->ptr) cudaFree(b->ptr);
+        b->ptr = nullptr;
+        b->bytes = 0;
+    }
+    tc_release_buffers();
+    return TLIBTTM_OK;
+}
+
+int tlibttm_k_order_layout(size_t* layout, size_t p, size_t k)
+{
+    if (!layout || p == 0) return fail(TLIBTTM_ERR_ARG, "Error in tlib::ttm::detail::compute_k_order: range provided by begin and end not correct!");
+    tlib::ttm::detail::compute_k_order_layout(layout, layout + p, k);
+    return TLIBTTM_OK;
+}
+
+size_t tlibttm_inverse_mode(const size_t* layout, size_t p, size_t mode)
+{
+    try {
+        return tlib::ttm::detail::inverse_mode(layout, layout + p, mode);
+    } catch (std::exception const& ex) {
+        g_err = ex.what();
+        return 0;
+    }
+}
+
+int tlibttm_strides(const size_t* shape, size_t p, const size_t* layout, size_t* strides)
+{
+    try {
+        tlib::ttm::detail::compute_strides(shape, shape + p, layout, strides);
+    } catch (std::exception const& ex) {
+        return fail(TLIBTTM_ERR_ARG, ex.what());
+    }
+    return TLIBTTM_OK;
+}
+
+}  // extern "C"

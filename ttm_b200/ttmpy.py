@@ -1,0 +1,237 @@
+"""Drop-in for the reference's Python binding ``ttmpy`` (ttmpy/src/wrapped_ttm.cpp).
+
+    from ttm_b200 import ttmpy as tp
+    C = tp.ttm(q, A, B)                 # mode-q product, q one-based
+    D = tp.ttms(q, A, Bs, "forward")    # multiply every mode except q
+
+Both functions run on the GPU through the C ABI (include/tlibttm.h); there is
+no CPU fallback. Inputs may be numpy arrays (results come back as numpy
+arrays, the call blocks) or torch CUDA tensors (results are torch CUDA
+tensors produced on the current torch stream, no host round trip).
+
+Same contract as the reference binding, plus three widenings:
+
+* float32 as well as float64 (the reference binds only double,
+  wrapped_ttm.cpp:229-230). Other dtypes are converted to float64, as
+  pybind11's ``array_t<double>`` does.
+* A's layout pi is read from its strides (a C-ordered array gives the
+  last-order layout the reference hard-codes, wrapped_ttm.cpp:45), so
+  transposed or permuted views are computed correctly without a copy; C gets
+  A's layout, as in the reference (wrapped_ttm.cpp:57-66).
+* B's own memory order is honoured (row- or column-major); the reference
+  assumes row-major (wrapped_ttm.cpp:46).
+
+Error behaviour follows the reference: its own checks raise ValueError with
+the same texts (wrapped_ttm.cpp:37-53, 90-127); checks of tlib::ttm raise
+RuntimeError with tlib's texts (include/tlib/ttm.h:65-90).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+
+try:  # torch is optional for numpy callers
+    import torch
+except Exception:  # noqa: BLE001
+    torch = None
+
+
+def _is_torch(x) -> bool:
+    return torch is not None and isinstance(x, torch.Tensor)
+
+
+def _layout_from_strides(shape, strides):
+    """One-based layout pi listing modes from smallest to largest stride (ties: higher mode first)."""
+    p = len(shape)
+    order = sorted(range(p), key=lambda r: (strides[r], -r))
+    return [r + 1 for r in order]
+
+
+def _dense_strides(shape, pi):
+    w = [1] * len(shape)
+    for r in range(1, len(shape)):
+        w[pi[r] - 1] = w[pi[r - 1] - 1] * shape[pi[r - 1] - 1]
+    return w
+
+
+def _dtype_id(dt) -> int:
+    return _lib.F32 if dt in (np.float32, getattr(torch, "float32", None)) else _lib.F64
+
+
+def _prec(precision) -> int:
+    if isinstance(precision, str):
+        return _lib.PRECISIONS[precision]
+    return int(precision)
+
+
+def _check_q_p(q, p, fn):
+    if p == 0:
+        if fn == "ttm":
+            raise ValueError("Error calling ttmpy::ttm: first input should be a tensor with order greater than zero.")
+        raise ValueError("Error calling ttmpy::ttms: input tensor order should be greater than zero.")
+
+
+def _ttm_numpy(q, A, B, precision):
+    A = np.asarray(A)
+    p = A.ndim
+    _check_q_p(q, p, "ttm")
+    if q == 0 or q > p:
+        raise ValueError("Error calling ttmpy::ttm: contraction mode should be greater than zero and at most equal to p.")
+    if A.dtype not in (np.float32, np.float64):
+        A = A.astype(np.float64)
+    B = np.asarray(B)
+    if B.ndim != 2:
+        raise ValueError("Error calling ttmpy::ttm: second input should be a mtrix with order equal to 2.")
+    if B.dtype != A.dtype:
+        B = B.astype(A.dtype)
+    if any(s < 0 for s in A.strides) or any(s % A.itemsize for s in A.strides):
+        A = np.ascontiguousarray(A)
+    if B.flags.c_contiguous:
+        pib = [2, 1]
+    elif B.flags.f_contiguous:
+        pib = [1, 2]
+    else:
+        B = np.ascontiguousarray(B)
+        pib = [2, 1]
+    na = list(A.shape)
+    wa = [s // A.itemsize for s in A.strides]
+    pia = _layout_from_strides(na, wa)
+    nb = list(B.shape)
+    nc = list(na)
+    nc[q - 1] = nb[0]
+    wc = _dense_strides(nc, pia)
+    C = np.lib.stride_tricks.as_strided(np.empty(int(np.prod(nc)), dtype=A.dtype), shape=nc,
+                                        strides=[w * A.itemsize for w in wc])
+    _lib.ttm_raw(_dtype_id(A.dtype.type), _prec(precision), q, p, A.ctypes.data, na, wa, pia,
+                 B.ctypes.data, nb, pib, C.ctypes.data, nc, wc, 0)
+    return C
+
+
+def _ttm_torch(q, A, B, precision):
+    p = A.dim()
+    _check_q_p(q, p, "ttm")
+    if q == 0 or q > p:
+        raise ValueError("Error calling ttmpy::ttm: contraction mode should be greater than zero and at most equal to p.")
+    if A.dtype not in (torch.float32, torch.float64):
+        A = A.to(torch.float64)
+    if not _is_torch(B):
+        B = torch.as_tensor(np.asarray(B), device=A.device)
+    if B.dim() != 2:
+        raise ValueError("Error calling ttmpy::ttm: second input should be a mtrix with order equal to 2.")
+    B = B.to(device=A.device, dtype=A.dtype)
+    if any(s < 0 for s in A.stride()):
+        A = A.contiguous()
+    if B.is_contiguous():
+        pib = [2, 1]
+    elif B.t().is_contiguous():
+        pib = [1, 2]
+    else:
+        B = B.contiguous()
+        pib = [2, 1]
+    na = list(A.shape)
+    wa = list(A.stride())
+    pia = _layout_from_strides(na, wa)
+    nb = list(B.shape)
+    nc = list(na)
+    nc[q - 1] = nb[0]
+    wc = _dense_strides(nc, pia)
+    C = torch.empty_strided(nc, wc, dtype=A.dtype, device=A.device)
+    stream = torch.cuda.current_stream(A.device).cuda_stream if A.is_cuda else 0
+    if A.is_cuda:
+        with torch.cuda.device(A.device):
+            _lib.ttm_raw(_dtype_id(A.dtype), _prec(precision), q, p, A.data_ptr(), na, wa, pia,
+                         B.data_ptr(), nb, pib, C.data_ptr(), nc, wc, stream)
+    else:
+        _lib.ttm_raw(_dtype_id(A.dtype), _prec(precision), q, p, A.data_ptr(), na, wa, pia,
+                     B.data_ptr(), nb, pib, C.data_ptr(), nc, wc, 0)
+    return C
+
+
+def ttm(q, A, B, precision="default"):
+    """Mode-q tensor-times-matrix product C = A x_q B (reference wrapped_ttm.cpp:23-76).
+
+    C(i1..j..ip) = sum_{iq} A(i1..iq..ip) * B(j, iq); q is one-based.
+    ``precision`` selects the arithmetic ("default", "plain", "bf16x3",
+    "fp8", "ozaki", "auto"); "default" is the library-wide setting (plain
+    unless changed).
+    """
+    q = int(q)
+    if _is_torch(A):
+        return _ttm_torch(q, A, B, precision)
+    return _ttm_numpy(q, A, B, precision)
+
+
+def _ttms_check(q, A, Bs, order):
+    if order not in ("optimal", "backward", "forward"):
+        raise ValueError("Error calling ttmpy::ttms: multiplication order should be either 'optimal', 'backward' or 'forward'.")
+    p = A.dim() if _is_torch(A) else np.asarray(A).ndim
+    if p == 0:
+        raise ValueError("Error calling ttmpy::ttms: input tensor order should be greater than zero.")
+    if len(Bs) != p - 1:
+        raise ValueError("Error calling ttmpy::ttms: number of input matrices is not equal to the tensor order - 1.")
+    if q == 0 or q > p:
+        raise ValueError("Error calling ttmpy::ttms: non-contraction mode should be greater than zero and at most equal to p.")
+    if not all((b.dim() if _is_torch(b) else np.asarray(b).ndim) == 2 for b in Bs):
+        raise ValueError("Error calling ttmpy::ttms: some of the input matrices are not matrices.")
+    na = list(A.shape)
+    nbs = [tuple(b.shape) for b in Bs]
+    # Same comparisons as wrapped_ttm.cpp:120-121. Like the reference, the
+    # matrix of mode q+1 is not compared here; a mismatch there surfaces as
+    # tlib's RuntimeError from the contraction itself.
+    ok1 = all(nbs[r][1] == na[r] for r in range(q - 1))
+    ok2 = all(nbs[r][1] == na[r + 1] for r in range(q, p - 1))
+    if not (ok1 and ok2):
+        raise ValueError("Error calling ttmpy::ttms: vector dimension is not compatible with the dimension of a tensor mode.")
+    return p
+
+
+def _ttms_sequence(q, p, Bs, order):
+    """(mode, matrix index) pairs in the reference's multiplication order (wrapped_ttm.cpp:132-218)."""
+    def bidx(r):  # matrix of mode r (one-based, r != q)
+        return r - 1 if r < q else r - 2
+
+    modes = [r for r in range(1, p + 1) if r != q]
+    if order == "forward":
+        seq = modes
+    elif order == "backward":
+        seq = modes[::-1]
+    else:
+        # ascending 1/n_k - 1/m_k for B_k of shape (m_k, n_k): shrinking products first
+        def key(r):
+            m_k, n_k = Bs[bidx(r)].shape
+            return 1.0 / float(n_k) - 1.0 / float(m_k)
+        seq = sorted(modes, key=key)
+    return [(r, bidx(r)) for r in seq]
+
+
+def ttms(q, A, Bs, order="forward", precision="default"):
+    """Multiply A by Bs[k] on every mode except q (reference wrapped_ttm.cpp:81-222).
+
+    ``order`` is "forward" (ascending modes), "backward" (descending) or
+    "optimal" (ascending 1/n_k - 1/m_k, i.e. the most shrinking factors first).
+    Numpy inputs are moved to the GPU once; all intermediates stay in device
+    memory and only the final tensor returns to the host.
+    """
+    q = int(q)
+    p = _ttms_check(q, A, Bs, order)
+    seq = _ttms_sequence(q, p, Bs, order)
+    if _is_torch(A):
+        c = A
+        for r, k in seq:
+            c = ttm(r, c, Bs[k], precision)
+        return c
+    if torch is None or not torch.cuda.is_available():
+        c = np.asarray(A)
+        for r, k in seq:
+            c = ttm(r, c, Bs[k], precision)
+        return c
+    A = np.asarray(A)
+    if A.dtype not in (np.float32, np.float64):
+        A = A.astype(np.float64)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    c = torch.from_numpy(np.ascontiguousarray(A)).to(dev)
+    for r, k in seq:
+        b = torch.from_numpy(np.ascontiguousarray(np.asarray(Bs[k], dtype=A.dtype))).to(dev)
+        c = ttm(r, c, b, precision)
+    return c.cpu().numpy()
