@@ -1,0 +1,392 @@
+"""Benchmark of the B200 mode-q TTM on the precision-study workload.
+
+Workload (one step): A of extents (S,S,S,S) fp32, first-order layout, N(0,1)
+entries (seed 0), contracted on every mode q = 1..4 with its own B_q of
+shape (S,S) (column-major, N(0,1)); C_q has A's shape. S = 256 by default:
+2^32 elements, 17.2 GB per tensor, so every launch streams far more than the
+126 MB L2 (no flush needed). Work per step = 4 * 2*m*N_A FLOP.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision P] [--size S]
+    python bench.py --impl reference ...   # the reference tlib::ttm on the host cores
+
+One JSON line on rank 0 (see the keys below). Under torchrun each rank runs
+the same workload on its own GPU (weak scaling, no data-path collective); the
+time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TTM TFLOP/s & %roofline, mixed-prec/batched vs plain FP32 at stated rel. error"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", default="auto", help="plain | bf16x3 | fp8 | auto")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(S):
+    return f"precision study: A {S}^4 fp32 first-order N(0,1), q=1..4, B_q ({S},{S}) col-major"
+
+
+def dense_strides(n, pi):
+    w = [1] * len(n)
+    for r in range(1, len(n)):
+        w[pi[r] - 1] = w[pi[r - 1] - 1] * n[pi[r - 1] - 1]
+    return w
+
+
+def flops_per_step(S):
+    return 4 * 2.0 * S * float(S) ** 4
+
+
+def bytes_per_ttm(S, es=4):
+    return es * (2.0 * float(S) ** 4 + S * S)
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm: tlib::ttm (combined policy) compiled with OpenBLAS, on the host cores
+# ---------------------------------------------------------------------------------------------
+def reference_sample_run(S, target_s, steps, warmup):
+    """Times the reference on a bounded sample of the workload: the same four contractions with the
+    non-contracted mode of largest position cut to `s` (so each TFLOP/s figure is measured on slices of
+    exactly the full problem's geometry). Returns (tflops_median, cores, sample_desc)."""
+    from oracle import Reference
+    ref = Reference()
+    cores = ref.cores
+    rng = np.random.default_rng(0)
+
+    def shapes(s):
+        out = []
+        for q in range(1, 5):
+            na = [S, S, S, s] if q < 4 else [s, S, S, S]
+            out.append((q, na))
+        return out
+
+    def run_step(s, bufs):
+        t = 0.0
+        for (q, na), (a, b, c) in zip(shapes(s), bufs):
+            pia = [1, 2, 3, 4]
+            nc = list(na)
+            nc[q - 1] = S
+            t0 = time.perf_counter()
+            ref.ttm(q, a, na, dense_strides(na, pia), pia, b, [S, na[q - 1]], [1, 2], c, nc,
+                    dense_strides(nc, pia))
+            t += time.perf_counter() - t0
+        return t
+
+    def make(s):
+        bufs = []
+        n = S * S * S * s
+        a = rng.standard_normal(n, dtype=np.float32)
+        for q, na in shapes(s):
+            b = rng.standard_normal(S * na[q - 1], dtype=np.float32)
+            c = np.empty(n, dtype=np.float32)
+            bufs.append((a, b, c))
+        return bufs
+
+    s = 2
+    t = run_step(s, make(s))
+    per_slice = t / s
+    s = int(max(2, min(S, target_s / max(per_slice, 1e-6))))
+    bufs = make(s)
+    for _ in range(warmup):
+        run_step(s, bufs)
+    times = [run_step(s, bufs) for _ in range(steps)]
+    flop = 4 * 2.0 * S * S * S * S * s
+    tf = [flop / t / 1e12 for t in times]
+    desc = (f"A ({S},{S},{S},{s}) for q=1..3 and ({s},{S},{S},{S}) for q=4, fp32, B ({S},{S}); "
+            f"{steps} timed steps of 4 TTMs, median; {cores} OpenMP/BLAS threads")
+    return statistics.median(tf), cores, desc, times
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    tf, cores, desc, times = reference_sample_run(args.size, target_s=4.0, steps=steps, warmup=max(0, args.warmup))
+    line = {
+        "metric": METRIC, "value": tf, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1), seed 0",
+        "impl": "reference",
+        "config": {"workload": workload_name(args.size), "sample": desc, "parallelism": "host cores"},
+        "cpu_baseline": {"value": tf, "unit": "TFLOP/s", "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": tf, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].isdigit():
+                    rows.append(f)
+        except Exception:  # noqa: BLE001
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace('.', '', 1).isdigit())
+                if any(r[3].replace('.', '', 1).isdigit() for r in rows) else None}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from ttm_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    S = args.size
+    prec = _lib.PRECISIONS[args.precision]
+    n = S ** 4
+    gen = torch.Generator(device=dev).manual_seed(0 + rank)
+    A = torch.randn(n, device=dev, generator=gen, dtype=torch.float32)
+    Bs = [torch.randn(S * S, device=dev, generator=gen, dtype=torch.float32) for _ in range(4)]
+    C = torch.empty(n, device=dev, dtype=torch.float32)
+    na = [S, S, S, S]
+    pia = [1, 2, 3, 4]
+    wa = dense_strides(na, pia)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    def ttm(q, out=C, a=A):
+        _lib.ttm_raw(_lib.F32, prec, q, 4, a.data_ptr(), na, wa, pia, Bs[q - 1].data_ptr(), [S, S], [1, 2],
+                     out.data_ptr(), na, wa, sh)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # correctness spot check of this exact configuration (sampled fibres vs float64) before timing
+    relerr = {}
+    rng = np.random.default_rng(123)
+    for q in range(1, 5):
+        ttm(q)
+        torch.cuda.synchronize(dev)
+        A4 = A.view(S, S, S, S)      # index [i4][i3][i2][i1] (first-order memory)
+        C4 = C.view(S, S, S, S)
+        Bq = Bs[q - 1].view(S, S).double().cpu().numpy()   # [l][j] : column-major (m, nq)
+        num = den = 0.0
+        worst = 0.0
+        for _ in range(24):
+            idx = [int(x) for x in rng.integers(0, S, size=4)]
+            sl = [slice(None) if (3 - d) == (q - 1) else idx[d] for d in range(4)]
+            fib = A4[tuple(sl)].double().cpu().numpy()
+            got = C4[tuple(sl)].double().cpu().numpy()
+            want = fib @ Bq
+            num += float(np.sum((got - want) ** 2))
+            den += float(np.sum(want ** 2))
+            worst = max(worst, float(np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-30))))
+        relerr[q] = (float(np.sqrt(num / den)), worst)
+    kernel_name = _lib.last_kernel()
+
+    for _ in range(max(3, args.warmup)):
+        for q in range(1, 5):
+            ttm(q)
+    barrier()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(4 * args.steps)]
+    launches0 = _lib.launch_count()
+    with ClockSampler(local) as clk:
+        barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        k = 0
+        for _ in range(args.steps):
+            for q in range(1, 5):
+                ev[k][0].record(stream)
+                ttm(q)
+                ev[k][1].record(stream)
+                k += 1
+        t1.record(stream)
+        barrier()
+    launches = _lib.launch_count() - launches0
+    elapsed = t0.elapsed_time(t1) / 1e3
+    if world > 1:
+        tt = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    per_launch = [s.elapsed_time(e) / 1e3 for s, e in ev]
+    clocks = clk.summary()
+
+    value = world * flops_per_step(S) * args.steps / elapsed / 1e12
+    hbm_peak, bf16_peak, peak_kind = measured_peaks()
+    avg_launch = statistics.mean(per_launch)
+    achieved_gbs = bytes_per_ttm(S) / avg_launch / 1e9
+
+    # plain-FP32 comparison number (same workload, exact FFMA path), one step
+    plain_tflops = None
+    if prec != _lib.PREC_PLAIN:
+        for q in range(1, 5):
+            _lib.ttm_raw(_lib.F32, _lib.PREC_PLAIN, q, 4, A.data_ptr(), na, wa, pia, Bs[q - 1].data_ptr(), [S, S],
+                         [1, 2], C.data_ptr(), na, wa, sh)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for q in range(1, 5):
+            _lib.ttm_raw(_lib.F32, _lib.PREC_PLAIN, q, 4, A.data_ptr(), na, wa, pia, Bs[q - 1].data_ptr(), [S, S],
+                         [1, 2], C.data_ptr(), na, wa, sh)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_tflops = flops_per_step(S) / (e0.elapsed_time(e1) / 1e3) / 1e12
+
+    # end to end through the C ABI with pinned host buffers: copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        hA = torch.empty(n, dtype=torch.float32, pin_memory=True)
+        hA.copy_(A)
+        hC = torch.empty(n, dtype=torch.float32, pin_memory=True)
+        hB = [b.cpu().pin_memory() for b in Bs]
+
+        def e2e_step():
+            for q in range(1, 5):
+                _lib.ttm_raw(_lib.F32, prec, q, 4, hA.data_ptr(), na, wa, pia, hB[q - 1].data_ptr(), [S, S], [1, 2],
+                             hC.data_ptr(), na, wa, sh)
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        barrier()
+        te = time.perf_counter() - t0
+        if world > 1:
+            tt = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": world * flops_per_step(S) * args.e2e_steps / te / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(4 * (4 * n + 4 * S * S)), "d2h_bytes_per_step": int(4 * 4 * n),
+               "steps": args.e2e_steps}
+        del hA, hC
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            tf, cores, desc, _ = reference_sample_run(S, target_s=2.0, steps=1, warmup=0)
+            cpu = {"value": tf, "unit": "TFLOP/s", "cores": cores, "kind": "reference", "sample": desc}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "TFLOP/s", "cores": None, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic N(0,1) (torch seed = rank)",
+            "config": {"workload": workload_name(S), "precision": args.precision, "kernel": kernel_name,
+                       "flop_per_step": flops_per_step(S), "parallelism": f"replicas x{world} (one per GPU)",
+                       "l2": "inputs (17.2 GB per tensor at S=256) exceed the 126 MB L2; no flush"},
+            "rel_error_vs_fp64": {f"q{q}": {"fro": relerr[q][0], "max": relerr[q][1]} for q in relerr},
+            "plain_fp32_tflops": plain_tflops,
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": kernel_name, "algorithmic_bytes_per_launch": bytes_per_ttm(S),
+                         "avg_launch_ms": 1e3 * avg_launch},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
