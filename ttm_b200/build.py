@@ -6,7 +6,8 @@
 Each .cu under ttm_b200/csrc is compiled separately (in parallel) with
 ``-gencode arch=compute_100a,code=sm_100a -lineinfo -O3`` and the objects are
 linked into ttm_b200/libtlibttm_cuda.so with the CUDA runtime linked
-statically, so the library has no dependency beyond the driver.
+statically; driver entry points (tensor-map encoding) are resolved at run
+time, so the library loads even where no driver is installed.
 """
 from __future__ import annotations
 
@@ -81,7 +82,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
         msg = "\n".join(f"--- {s}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     tmp = LIB + ".tmp"
-    cmd = [cc] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static", "-lcuda"]
+    cmd = [cc] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static"]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)

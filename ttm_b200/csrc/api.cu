@@ -329,6 +329,8 @@ int run(const Args& x, int precision, void* stream)
     if (wc == Where::Host)
         if ((e = cudaMemcpyAsync(x.c, d.c, pl.c_elems * es, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "copy of C");
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    if (tc_read_status())
+        return fail(TLIBTTM_ERR_DEVICE, "tlibttm: a tensor-core kernel gave up on a bounded wait; its output is invalid.");
     return TLIBTTM_OK;
 }
 
@@ -388,7 +390,10 @@ unsigned long long tlibttm_launch_count(int reset)
 int tlibttm_synchronize(void* stream)
 {
     cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
-    return e == cudaSuccess ? TLIBTTM_OK : cuda_fail(e, "cudaStreamSynchronize");
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    if (tc_read_status())
+        return fail(TLIBTTM_ERR_DEVICE, "tlibttm: a tensor-core kernel gave up on a bounded wait; its output is invalid.");
+    return TLIBTTM_OK;
 }
 
 int tlibttm_release_buffers(void)

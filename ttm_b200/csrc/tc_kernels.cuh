@@ -12,7 +12,10 @@ bool tc_supported(const View3& v, int precision);
 // identifier of the main kernel launched.
 cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid);
 
-// Frees device scratch owned by the tensor-core paths on the current device.
+// Frees device state owned by the tensor-core paths on the current device.
 void tc_release_buffers();
+
+// Reads and clears the device status word (non-zero: a kernel gave up on a bounded wait).
+int tc_read_status();
 
 }  // namespace tlibttm
