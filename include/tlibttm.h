@@ -104,6 +104,36 @@ int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p,
                    void* c, const size_t* nc, const size_t* wc,
                    void* stream);
 
+/*
+ * No counterpart in the reference: the bf16x3 contraction (as tlibttm_ttm_ex with
+ * TLIBTTM_F32 / TLIBTTM_PREC_BF16X3) for callers that cannot let a library
+ * allocate device memory — a host application whose allocator already owns the
+ * device's memory, a latency-bound loop that must not risk the implicit device
+ * synchronisation of cudaMalloc/cudaFree, or a process under a fixed memory
+ * budget. It allocates nothing: its scratch (the bf16 hi/lo image of B and a
+ * status word) lives in file-scope device arrays that every GPU loading the
+ * library holds until exit.
+ *
+ * Limits: a, b and c must all be device memory of the current device (no host
+ * staging); A and C dense under their layout; m > 16 and either inner % 4 == 0
+ * or q == pia[0] with n_q % 4 == 0; and the B image,
+ * ceil(m/16)*16 * ceil(n_q/32)*32 * 4 bytes, at most 1 MiB (for example
+ * m = 256 with n_q <= 1024). Larger or unsupported problems are rejected with
+ * TLIBTTM_ERR_ARG / TLIBTTM_ERR_UNSUPPORTED and a message; nothing is launched.
+ *
+ * The work is enqueued on `stream`; tlibttm_synchronize reports a failed
+ * bounded wait of its kernels. The first call on each device performs a
+ * one-time set-up there (it looks up the arrays' device addresses); make that
+ * first call before any stream capture. All calls share the arrays, so calls
+ * whose work overlaps on the GPU (different streams or host threads) race and
+ * must be serialised by the caller.
+ */
+int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p,
+                                   const float* a, const size_t* na, const size_t* wa, const size_t* pia,
+                                   const float* b, const size_t* nb, const size_t* pib,
+                                   float* c, const size_t* nc, const size_t* wc,
+                                   void* stream);
+
 /* Text of the last error reported on the calling thread ("" if none). */
 const char* tlibttm_last_error(void);
 

@@ -40,6 +40,8 @@ def _declare(L):
         f.argtypes = sig
     L.tlibttm_ttm_ex.restype = C.c_int
     L.tlibttm_ttm_ex.argtypes = [C.c_int, C.c_int] + sig
+    L.tlibttm_ttm_f32_bf16x3_noalloc.restype = C.c_int
+    L.tlibttm_ttm_f32_bf16x3_noalloc.argtypes = sig
     L.tlibttm_last_error.restype = C.c_char_p
     L.tlibttm_last_kernel.restype = C.c_char_p
     L.tlibttm_set_precision.restype = C.c_int

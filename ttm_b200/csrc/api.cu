@@ -368,6 +368,45 @@ int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p, const void*
     return run(x, precision, stream);
 }
 
+// No counterpart in the reference: the bf16x3 contraction without any device
+// allocation (declaration and contract in include/tlibttm.h).
+int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const size_t* na, const size_t* wa,
+                                   const size_t* pia, const float* b, const size_t* nb, const size_t* pib, float* c,
+                                   const size_t* nc, const size_t* wc, void* stream)
+{
+    Args x{TLIBTTM_F32, q, p, a, na, wa, pia, b, nb, pib, c, nc, wc};
+    int rc = validate(x);
+    if (rc) return rc;
+    Plan pl;
+    if ((rc = make_plan(x, pl))) return rc;
+    if (!pl.dense)
+        return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm_ttm_f32_bf16x3_noalloc: A and C must be dense under their layout.");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    Where wa_, wb_, wc_;
+    if ((rc = classify(x.a, dev, wa_)) || (rc = classify(x.b, dev, wb_)) || (rc = classify(x.c, dev, wc_))) return rc;
+    if (wa_ != Where::Device || wb_ != Where::Device || wc_ != Where::Device)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_f32_bf16x3_noalloc: a, b and c must be device memory "
+                                     "(host operands would need staging buffers).");
+    View3 v = pl.v;
+    v.a = x.a;
+    v.b = x.b;
+    v.c = x.c;
+    if (!tc_supported(v, TLIBTTM_PREC_BF16X3))
+        return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm_ttm_f32_bf16x3_noalloc: shape not handled by the tensor-core "
+                                             "kernel (needs m > 16, and inner % 4 == 0 or q = pi_1 with n_q % 4 == 0).");
+    if (tc_image_bytes(v) > kNoAllocImageBytes)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_f32_bf16x3_noalloc: B needs a " + std::to_string(tc_image_bytes(v)) +
+                                         "-byte split image; this entry point holds at most " +
+                                         std::to_string(kNoAllocImageBytes) +
+                                         " bytes (ceil(m/16)*16 * ceil(n_q/32)*32 * 4 bytes, e.g. m = 256 with n_q <= 1024).");
+    int kid = K_NONE;
+    e = launch_tc_noalloc(v, static_cast<cudaStream_t>(stream), &kid);
+    if (e == cudaSuccess) ++g_launches;   // split_b_kernel; note_launch counts the main kernel
+    return note_launch(e, kid);
+}
+
 const char* tlibttm_last_error(void) { return g_err.c_str(); }
 
 int tlibttm_set_precision(int precision)
@@ -393,6 +432,8 @@ int tlibttm_synchronize(void* stream)
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
     if (tc_read_status())
         return fail(TLIBTTM_ERR_DEVICE, "tlibttm: a tensor-core kernel gave up on a bounded wait; its output is invalid.");
+    if (tc_read_noalloc_status())
+        return fail(TLIBTTM_ERR_DEVICE, "tlibttm: the last allocation-free bf16x3 launch gave up on a bounded wait.");
     return TLIBTTM_OK;
 }
 

@@ -682,6 +682,118 @@ cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid)
     return e;
 }
 
+// ------------------------------------------------------------------ allocation-free variant
+// The bf16x3 path above takes its pre-split B image from the stream-ordered pool
+// (cudaMallocAsync). Some callers cannot let a library allocate device memory: a
+// host application whose own allocator has reserved the device's memory, a
+// latency-bound loop that must not risk the implicit device synchronisation of
+// cudaMalloc/cudaFree, or a process running under a fixed device-memory budget.
+// For them, launch_tc_noalloc runs the same kernels with the B image in this
+// file-scope array. Every GPU that loads the library holds the array until exit.
+// All calls share it and it keeps the previous call's contents: split_b_kernel
+// rewrites every byte a launch reads (zero padding included), and the status
+// word is cleared before each launch. Calls whose work overlaps on the GPU (two
+// streams, or two host threads) race on the array and must be serialised.
+static __device__ __align__(256) uint8_t g_noalloc_image[kNoAllocImageBytes];
+static __device__ __align__(256) int g_noalloc_status[64];
+
+struct NoAllocSymbols {
+    uint8_t* image = nullptr;
+    int* status = nullptr;
+};
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocSymbols g_noalloc_syms[kMaxDevices];
+
+// Device addresses of the two arrays on device `dev` (the current device), looked
+// up once per device. In host code the array names are host-side stand-ins, not
+// device addresses, so kernels only ever receive the looked-up pointers.
+cudaError_t noalloc_symbols(int dev, NoAllocSymbols& out)
+{
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocSymbols& sy = g_noalloc_syms[dev];
+    if (!sy.image) {
+        void* img = nullptr;
+        void* st = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&img, g_noalloc_image);
+        if (e != cudaSuccess) return e;
+        e = cudaGetSymbolAddress(&st, g_noalloc_status);
+        if (e != cudaSuccess) return e;
+        sy.image = static_cast<uint8_t*>(img);
+        sy.status = static_cast<int*>(st);
+    }
+    out = sy;
+    return cudaSuccess;
+}
+
+size_t tc_image_bytes(const View3& v)
+{
+    const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
+    const int64_t jblocks = (v.m + nt - 1) / nt;
+    const int64_t kchunks = (v.nq + kBK - 1) / kBK;
+    return (size_t)(jblocks * kchunks * 2) * smem_layout(nt).b_bytes;
+}
+
+cudaError_t launch_tc_noalloc(const View3& v, cudaStream_t s, int* kid)
+{
+    *kid = K_TC_BF16X3;
+    if (tc_image_bytes(v) > kNoAllocImageBytes) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    NoAllocSymbols sy;
+    if ((e = noalloc_symbols(dev, sy)) != cudaSuccess) return e;
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+
+    const int geom = geometry_of(v);
+    const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
+    const int jblocks = (int)((v.m + nt - 1) / nt);
+    const int kchunks = (int)((v.nq + kBK - 1) / kBK);
+    const SmemLayout L = smem_layout(nt);
+
+    CUtensorMap amap;
+    if (!encode_a_map(v, geom, &amap)) return cudaErrorInvalidValue;
+    if ((e = cudaMemsetAsync(sy.status, 0, sizeof(int), s)) != cudaSuccess) return e;
+
+    TcParams P{};
+    P.c = static_cast<float*>(v.c);
+    P.bimg = sy.image;
+    P.status = sy.status;
+    P.outer = v.outer;
+    P.nq = v.nq;
+    P.inner = v.inner;
+    P.m = v.m;
+    P.tiles_m = geom == GEOM_MN ? v.outer * ((v.inner + kBM - 1) / kBM) : (v.outer + kBM - 1) / kBM;
+    P.tiles = P.tiles_m * jblocks;
+    P.nt = nt;
+    P.jblocks = jblocks;
+    P.kchunks = kchunks;
+    P.vec_c = (geom == GEOM_K) && (v.m % 4 == 0) && ((reinterpret_cast<uintptr_t>(v.c) & 15u) == 0);
+    const size_t ctrl = 1024;
+    int stages = (int)((227 * 1024 - 1024 - ctrl) / L.stage_bytes);
+    if (stages > kMaxStages) stages = kMaxStages;
+    if (stages < 2) return cudaErrorNotSupported;
+    P.stages = stages;
+    const size_t smem = 1024 + (size_t)stages * L.stage_bytes + ctrl;
+
+    const int64_t total = (int64_t)jblocks * kchunks * nt * 4;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks, kchunks,
+                                          sy.image);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int grid = (int)std::min<int64_t>(P.tiles, sms);
+    if (geom == GEOM_MN) {
+        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_MN><<<grid, kThreads, smem, s>>>(amap, P);
+    } else {
+        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_K><<<grid, kThreads, smem, s>>>(amap, P);
+    }
+    return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
 int tc_read_status()
 {
     int dev = 0;
@@ -692,6 +804,22 @@ int tc_read_status()
     int st = 0;
     if (cudaMemcpy(&st, it->second.status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
     if (st) cudaMemset(it->second.status, 0, sizeof(int));
+    return st;
+}
+
+int tc_read_noalloc_status()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 0;
+    int* p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        p = g_noalloc_syms[dev].status;
+    }
+    if (!p) return 0;
+    int st = 0;
+    if (cudaMemcpy(&st, p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+    if (st) cudaMemset(p, 0, sizeof(int));
     return st;
 }
 

@@ -18,4 +18,18 @@ void tc_release_buffers();
 // Reads and clears the device status word (non-zero: a kernel gave up on a bounded wait).
 int tc_read_status();
 
+// Largest pre-split B image the allocation-free bf16x3 variant can hold (bytes):
+// ceil(m/16)*16 * ceil(n_q/32)*32 * 4 <= 1 MiB for m <= 256, e.g. m = 256 with n_q <= 1024.
+constexpr size_t kNoAllocImageBytes = size_t(1) << 20;
+
+// Bytes of the pre-split B image a bf16x3 launch of this view needs.
+size_t tc_image_bytes(const View3& v);
+
+// The bf16x3 path with its scratch in file-scope device arrays: allocates no memory.
+// Returns cudaErrorInvalidValue when the B image exceeds kNoAllocImageBytes.
+cudaError_t launch_tc_noalloc(const View3& v, cudaStream_t s, int* kid);
+
+// Status word of the allocation-free variant (non-zero: its last launch gave up on a bounded wait).
+int tc_read_noalloc_status();
+
 }  // namespace tlibttm
