@@ -27,6 +27,7 @@
 #include <cuda_bf16.h>
 
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <unordered_map>
 
@@ -36,11 +37,12 @@
 namespace tlibttm {
 namespace {
 
-constexpr int kThreads = 320;
+constexpr int kConvWarps = 8;                   // converter warps
+constexpr int kThreads = (2 + kConvWarps + 4) * 32;  // producer, MMA, converters, 4 epilogue warps
+constexpr int kConvThreads = kConvWarps * 32;
 constexpr int kBM = 128;       // MMA M
-constexpr int kBK = 32;        // l per stage
+constexpr int kBK = 16;        // l per stage (one MMA K step)
 constexpr int kMaxNT = 256;    // MMA N max
-constexpr int kMaxStages = 6;
 constexpr unsigned long long kTimeoutNs = 4000000000ull;
 
 enum { GEOM_MN = 0, GEOM_K = 1 };
@@ -134,7 +136,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
     d |= (uint64_t)(layout & 7u) << 61;
     return d;
 }
-constexpr uint32_t kLayoutSW128 = 2, kLayoutSW64 = 4;
+constexpr uint32_t kLayoutSW128 = 2, kLayoutSW32 = 6;
 
 // Instruction descriptor, kind::f16: D f32, A/B bf16, B K-major, M = 128.
 __host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn_major)
@@ -183,14 +185,15 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_
     lo = *reinterpret_cast<uint32_t*>(&l);
 }
 
-// Byte offset of a 16-byte chunk inside a K-major SW64 bf16 tile with 64-byte rows (32 l per row).
-__host__ __device__ __forceinline__ uint32_t kmaj_sw64_off(uint32_t row, uint32_t chunk)
+// Byte offset of a 16-byte chunk inside a K-major SW32 bf16 tile with 32-byte rows (16 l per row):
+// 8-row atoms of 256 B, chunk bit XOR-ed with row bit 2 (the 32-byte swizzle).
+__host__ __device__ __forceinline__ uint32_t kmaj_sw32_off(uint32_t row, uint32_t chunk)
 {
-    return (row >> 3) * 512u + (row & 7u) * 64u + ((chunk ^ ((row >> 1) & 3u)) << 4);
+    return (row >> 3) * 256u + (row & 7u) * 32u + ((chunk ^ ((row >> 2) & 1u)) << 4);
 }
 
 // Byte offset of a 16-byte chunk (8 consecutive MN elements) in an MN-major SW128 bf16 tile of
-// 128 MN x 32 K laid out as [K group of 8][MN block of 64][8 K rows][64 MN].
+// 128 MN x 16 K laid out as [K group of 8][MN block of 64][8 K rows][64 MN].
 __device__ __forceinline__ uint32_t mnmaj_sw128_off(uint32_t l, uint32_t ichunk)
 {
     const uint32_t atom = (l >> 3) * 2u + (ichunk >> 3);
@@ -198,9 +201,27 @@ __device__ __forceinline__ uint32_t mnmaj_sw128_off(uint32_t l, uint32_t ichunk)
     return atom * 1024u + row * 128u + ((c ^ row) << 4);
 }
 
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int c0, int c1)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"
+                 ::"l"(map), "r"(su32(src)), "r"(c0), "r"(c1)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int c0, int c1, int c2)
+{
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+                 ::"l"(map), "r"(su32(src)), "r"(c0), "r"(c1), "r"(c2)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 struct TcParams {
     float* c;
-    const uint8_t* bimg;     // pre-split B: [jb][kc][hi|lo][NT rows x 64 B]
+    const uint8_t* bimg;     // pre-split B: [jb][kc][hi|lo][NT rows x 32 B]
     int* status;             // device status word (0 = ok)
     int64_t outer, nq, inner, m;
     int64_t tiles_m;         // M tiles per j block
@@ -208,54 +229,87 @@ struct TcParams {
     int nt;                  // MMA N (multiple of 16, <= 256)
     int jblocks;
     int kchunks;
-    int stages;
-    int vec_c;               // GEOM_K epilogue may use 16-byte stores
+    int fstages;             // FP32 staging ring depth
+    int ostages;             // bf16 operand ring depth
+    int tma_c;               // epilogue stores C through the C tensor map
 };
 
+// Shared memory: [FP32 ring][operand ring: (A_hi, A_lo, B_hi, B_lo) per stage][epilogue staging][barriers].
 struct SmemLayout {
-    uint32_t f32_bytes, abf_bytes, b_bytes, stage_bytes;
+    uint32_t f32_bytes, abf_bytes, b_bytes, op_bytes;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int nt)
 {
     SmemLayout L;
-    L.f32_bytes = kBM * kBK * 4;            // 16 KB
-    L.abf_bytes = kBM * kBK * 2;            // 8 KB per part
-    L.b_bytes = (uint32_t)nt * kBK * 2;     // per part
-    L.stage_bytes = L.f32_bytes + 2 * L.abf_bytes + 2 * L.b_bytes;
+    L.f32_bytes = kBM * kBK * 4;            // 8 KB
+    L.abf_bytes = kBM * kBK * 2;            // 4 KB per part
+    L.b_bytes = (uint32_t)nt * kBK * 2;     // per part, multiple of 512
+    L.op_bytes = 2 * L.abf_bytes + 2 * L.b_bytes;
     return L;
 }
 
+constexpr int kMaxF = 16, kMaxO = 4;
+constexpr uint32_t kEpiBuf = 32 * 32 * 4;        // one 32 x 32 fp32 staging tile
+constexpr uint32_t kEpiBytes = 4 * 2 * kEpiBuf;  // 4 epilogue warps, double-buffered
+constexpr size_t kCtrlBytes = 1024;
+constexpr size_t kSmemBudget = 227 * 1024;
+
+// Ring depths for a given N tile; false if the minimum does not fit.
+__host__ inline bool choose_stages(int nt, int& fs, int& os, size_t& smem)
+{
+    const SmemLayout L = smem_layout(nt);
+    const size_t avail = kSmemBudget - 1024 - kCtrlBytes - kEpiBytes;
+    os = kMaxO;
+    while (os > 2 && (size_t)os * L.op_bytes + 6 * L.f32_bytes > avail) --os;
+    if ((size_t)os * L.op_bytes + 6 * L.f32_bytes > avail) return false;
+    fs = (int)((avail - (size_t)os * L.op_bytes) / L.f32_bytes);
+    if (fs > kMaxF) fs = kMaxF;
+    smem = 1024 + (size_t)fs * L.f32_bytes + (size_t)os * L.op_bytes + kEpiBytes + kCtrlBytes;
+    return true;
+}
+
+__device__ __forceinline__ uint4 pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) { return make_uint4(a, b, c, d); }
+
 template <int GEOM>
-__global__ void __launch_bounds__(kThreads, 1) tc_bf16x3_kernel(const __grid_constant__ CUtensorMap amap, TcParams P)
+__global__ void __launch_bounds__(kThreads, 1)
+    tc_bf16x3_kernel(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap cmap, TcParams P)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    // 1024-byte aligned base (swizzle atoms are address-based).
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const SmemLayout L = smem_layout(P.nt);
-    const int S = P.stages;
-    uint8_t* ctrl = smem + (size_t)S * L.stage_bytes;
-    uint64_t* full = reinterpret_cast<uint64_t*>(ctrl);           // [S]
-    uint64_t* conv = full + S;                                      // [S]
-    uint64_t* empty = conv + S;                                     // [S]
-    uint64_t* acc_full = empty + S;                                 // [2]
-    uint64_t* acc_empty = acc_full + 2;                             // [2]
-    uint64_t* drain = acc_empty + 2;                                // [1]
+    const int FS = P.fstages, OS = P.ostages;
+    uint8_t* fring = smem;
+    uint8_t* oring = smem + (size_t)FS * L.f32_bytes;
+    uint8_t* epi = oring + (size_t)OS * L.op_bytes;
+    uint8_t* ctrl = epi + kEpiBytes;
+    uint64_t* f_full = reinterpret_cast<uint64_t*>(ctrl);   // [FS]  TMA of A landed
+    uint64_t* f_empty = f_full + kMaxF;                       // [FS]  converters done reading
+    uint64_t* b_full = f_empty + kMaxF;                       // [OS]  B image landed
+    uint64_t* o_full = b_full + kMaxO;                        // [OS]  converted A written
+    uint64_t* o_empty = o_full + kMaxO;                       // [OS]  MMAs done reading
+    uint64_t* acc_full = o_empty + kMaxO;                     // [2]
+    uint64_t* acc_empty = acc_full + 2;                       // [2]
+    uint64_t* drain = acc_empty + 2;                          // [1]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    auto stage_f32 = [&](int s) { return smem + (size_t)s * L.stage_bytes; };
-    auto stage_ahi = [&](int s) { return stage_f32(s) + L.f32_bytes; };
-    auto stage_alo = [&](int s) { return stage_ahi(s) + L.abf_bytes; };
-    auto stage_bhi = [&](int s) { return stage_alo(s) + L.abf_bytes; };
-    auto stage_blo = [&](int s) { return stage_bhi(s) + L.b_bytes; };
+    auto f32_at = [&](int s) { return fring + (size_t)s * L.f32_bytes; };
+    auto ahi_at = [&](int s) { return oring + (size_t)s * L.op_bytes; };
+    auto alo_at = [&](int s) { return ahi_at(s) + L.abf_bytes; };
+    auto bhi_at = [&](int s) { return alo_at(s) + L.abf_bytes; };
+    auto blo_at = [&](int s) { return bhi_at(s) + L.b_bytes; };
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&conv[s], 4);
-            mbar_init(&empty[s], 1);
+        for (int s = 0; s < FS; ++s) {
+            mbar_init(&f_full[s], 1);
+            mbar_init(&f_empty[s], kConvWarps);
+        }
+        for (int s = 0; s < OS; ++s) {
+            mbar_init(&b_full[s], 1);
+            mbar_init(&o_full[s], kConvWarps);
+            mbar_init(&o_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
@@ -277,40 +331,36 @@ __global__ void __launch_bounds__(kThreads, 1) tc_bf16x3_kernel(const __grid_con
 
     const int64_t tiles = P.tiles;
     const int kchunks = P.kchunks;
-    const uint32_t tx_bytes = L.f32_bytes + 2 * L.b_bytes;
+    const int64_t mper = (P.inner + kBM - 1) / kBM;
 
     if (warp == 0) {
-        // ------------------------------------------------------------- TMA producer
+        // ------------------------------------------------------------- A producer (TMA)
         if (lane == 0) {
             int s = 0;
             uint32_t ph = 0;
             bool ok = true;
-            int issued[kMaxStages];
-            for (int i = 0; i < kMaxStages; ++i) issued[i] = -1;
+            int issued[kMaxF];
+            for (int i = 0; i < kMaxF; ++i) issued[i] = -1;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                const int64_t jb = t / P.tiles_m, mt = t - jb * P.tiles_m;
+                const int64_t mt = t % P.tiles_m;
                 for (int kc = 0; kc < kchunks; ++kc) {
-                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(&f_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&full[s], tx_bytes);
+                    mbar_expect_tx(&f_full[s], L.f32_bytes);
                     if (GEOM == GEOM_MN) {
-                        const int64_t mper = (P.inner + kBM - 1) / kBM;
                         const int64_t k = mt / mper, ib = mt - k * mper;
-                        tma_load_3d(stage_f32(s), &amap, &full[s], (int)(ib * kBM), kc * kBK, (int)k);
+                        tma_load_3d(f32_at(s), &amap, &f_full[s], (int)(ib * kBM), kc * kBK, (int)k);
                     } else {
-                        tma_load_2d(stage_f32(s), &amap, &full[s], kc * kBK, (int)(mt * kBM));
+                        tma_load_2d(f32_at(s), &amap, &f_full[s], kc * kBK, (int)(mt * kBM));
                     }
-                    const uint8_t* img = P.bimg + ((size_t)(jb * kchunks + kc) * 2) * L.b_bytes;
-                    bulk_load(stage_bhi(s), img, L.b_bytes, &full[s]);
-                    bulk_load(stage_blo(s), img + L.b_bytes, L.b_bytes, &full[s]);
-                    if (++s == S) { s = 0; ph ^= 1; }
+                    if (++s == FS) { s = 0; ph ^= 1; }
                 }
             }
-            // Drain: none of this CTA's bulk copies may still be in flight when it exits.
-            for (int i = 0; i < S; ++i) {
+            // None of this CTA's bulk copies may still be in flight when it exits.
+            for (int i = 0; i < FS; ++i) {
                 if (issued[i] < 0) continue;
                 const unsigned long long t0 = gtimer();
-                while (!mbar_try(&full[i], (uint32_t)issued[i]) && gtimer() - t0 < kTimeoutNs) {}
+                while (!mbar_try(&f_full[i], (uint32_t)issued[i]) && gtimer() - t0 < kTimeoutNs) {}
             }
         }
     } else if (warp == 1) {
@@ -327,29 +377,26 @@ __global__ void __launch_bounds__(kThreads, 1) tc_bf16x3_kernel(const __grid_con
                 tc_fence_after();
                 const uint32_t dcol = tmem_base + (uint32_t)(ab * P.nt);
                 for (int kc = 0; kc < kchunks; ++kc) {
-                    if (!mbar_wait(&conv[s], ph, abort_flag)) { ok = false; break; }
-                    tc_fence_after();
-                    const uint32_t ahi = su32(stage_ahi(s)), alo = su32(stage_alo(s));
-                    const uint32_t bhi = su32(stage_bhi(s)), blo = su32(stage_blo(s));
-#pragma unroll
-                    for (int kk = 0; kk < kBK / 16; ++kk) {
-                        uint64_t dahi, dalo;
-                        if (GEOM == GEOM_MN) {
-                            dahi = smem_desc(ahi + kk * 4096u, 1024u, 2048u, kLayoutSW128);
-                            dalo = smem_desc(alo + kk * 4096u, 1024u, 2048u, kLayoutSW128);
-                        } else {
-                            dahi = smem_desc(ahi + kk * 32u, 16u, 512u, kLayoutSW64);
-                            dalo = smem_desc(alo + kk * 32u, 16u, 512u, kLayoutSW64);
-                        }
-                        const uint64_t dbhi = smem_desc(bhi + kk * 32u, 16u, 512u, kLayoutSW64);
-                        const uint64_t dblo = smem_desc(blo + kk * 32u, 16u, 512u, kLayoutSW64);
-                        const uint32_t first = (kc == 0 && kk == 0) ? 0u : 1u;
-                        mma_bf16(dcol, dahi, dbhi, idesc, first);
-                        mma_bf16(dcol, dahi, dblo, idesc, 1u);
-                        mma_bf16(dcol, dalo, dbhi, idesc, 1u);
+                    if (!mbar_wait(&b_full[s], ph, abort_flag) || !mbar_wait(&o_full[s], ph, abort_flag)) {
+                        ok = false;
+                        break;
                     }
-                    mma_commit(&empty[s]);     // stage free once these MMAs have read it
-                    if (++s == S) { s = 0; ph ^= 1; }
+                    tc_fence_after();
+                    uint64_t dahi, dalo;
+                    if (GEOM == GEOM_MN) {
+                        dahi = smem_desc(su32(ahi_at(s)), 1024u, 2048u, kLayoutSW128);
+                        dalo = smem_desc(su32(alo_at(s)), 1024u, 2048u, kLayoutSW128);
+                    } else {
+                        dahi = smem_desc(su32(ahi_at(s)), 16u, 256u, kLayoutSW32);
+                        dalo = smem_desc(su32(alo_at(s)), 16u, 256u, kLayoutSW32);
+                    }
+                    const uint64_t dbhi = smem_desc(su32(bhi_at(s)), 16u, 256u, kLayoutSW32);
+                    const uint64_t dblo = smem_desc(su32(blo_at(s)), 16u, 256u, kLayoutSW32);
+                    mma_bf16(dcol, dahi, dbhi, idesc, kc == 0 ? 0u : 1u);
+                    mma_bf16(dcol, dahi, dblo, idesc, 1u);
+                    mma_bf16(dcol, dalo, dbhi, idesc, 1u);
+                    mma_commit(&o_empty[s]);   // operand stage free once these MMAs have read it
+                    if (++s == OS) { s = 0; ph ^= 1; }
                 }
                 if (!ok) break;
                 mma_commit(&acc_full[ab]);     // accumulator ready for the epilogue
@@ -360,97 +407,137 @@ __global__ void __launch_bounds__(kThreads, 1) tc_bf16x3_kernel(const __grid_con
             const unsigned long long t0 = gtimer();
             while (!mbar_try(drain, 0) && gtimer() - t0 < kTimeoutNs) {}
         }
-    } else if (warp < 6) {
-        // ------------------------------------------------------------- converters
-        const int ct = threadIdx.x - 64;   // 0..127
-        int s = 0;
-        uint32_t ph = 0;
+    } else if (warp < 2 + kConvWarps) {
+        // ------------------------------------------------------------- converters (+ B loads)
+        const int ct = threadIdx.x - 64;   // 0 .. kConvThreads-1
+        const bool b_issuer = ct == 0;
+        const bool odd = lane & 1;
+        int fs = 0, os = 0;
+        uint32_t fph = 0, oph = 0;
         bool ok = true;
+        int b_issued[kMaxO];
+        for (int i = 0; i < kMaxO; ++i) b_issued[i] = -1;
         for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+            const int64_t jb = t / P.tiles_m;
             for (int kc = 0; kc < kchunks; ++kc) {
-                if (!mbar_wait(&full[s], ph, abort_flag)) { ok = false; break; }
-                const float* f = reinterpret_cast<const float*>(stage_f32(s));
-                uint8_t* ahi = stage_ahi(s);
-                uint8_t* alo = stage_alo(s);
+                if (!mbar_wait(&o_empty[os], oph ^ 1, abort_flag)) { ok = false; break; }
+                if (b_issuer) {
+                    b_issued[os] = (int)oph;
+                    mbar_expect_tx(&b_full[os], 2 * L.b_bytes);
+                    const uint8_t* img = P.bimg + ((size_t)(jb * kchunks + kc) * 2) * L.b_bytes;
+                    bulk_load(bhi_at(os), img, L.b_bytes, &b_full[os]);
+                    bulk_load(blo_at(os), img + L.b_bytes, L.b_bytes, &b_full[os]);
+                }
+                if (!mbar_wait(&f_full[fs], fph, abort_flag)) { ok = false; break; }
+                const uint8_t* f = f32_at(fs);
+                uint8_t* ahi = ahi_at(os);
+                uint8_t* alo = alo_at(os);
 #pragma unroll
-                for (int it = 0; it < 4; ++it) {
-                    const int u = ct + 128 * it;
-                    float4 x0, x1;
+                for (int it = 0; it < (kBM * kBK / 4) / kConvThreads; ++it) {
+                    const int v = ct + kConvThreads * it;   // float4 index within the 8 KB tile
+                    float4 x;
                     uint32_t off;
                     if (GEOM == GEOM_MN) {
-                        const int l = u >> 4, ic = u & 15;           // fp32 tile [32 l][128 i], rows of 512 B
-                        const float4* src = reinterpret_cast<const float4*>(f + l * kBM + ic * 8);
-                        x0 = src[0];
-                        x1 = src[1];
-                        off = mnmaj_sw128_off(l, ic);
+                        const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
+                        x = *reinterpret_cast<const float4*>(f + l * 512 + w * 16);
+                        off = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
                     } else {
-                        const int k = u >> 2, c = u & 3;             // fp32 tile [128 k][32 l], TMA SW128
-                        const uint32_t base = (uint32_t)k * 128u;
-                        const uint32_t c0 = (uint32_t)(2 * c), c1 = (uint32_t)(2 * c + 1);
-                        x0 = *reinterpret_cast<const float4*>(reinterpret_cast<const uint8_t*>(f) + base + ((c0 ^ (k & 7)) << 4));
-                        x1 = *reinterpret_cast<const float4*>(reinterpret_cast<const uint8_t*>(f) + base + ((c1 ^ (k & 7)) << 4));
-                        off = kmaj_sw64_off((uint32_t)k, (uint32_t)c);
+                        const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
+                        x = *reinterpret_cast<const float4*>(f + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                        off = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
                     }
-                    uint4 h, lo;
-                    split2(x0.x, x0.y, h.x, lo.x);
-                    split2(x0.z, x0.w, h.y, lo.y);
-                    split2(x1.x, x1.y, h.z, lo.z);
-                    split2(x1.z, x1.w, h.w, lo.w);
-                    *reinterpret_cast<uint4*>(ahi + off) = h;
-                    *reinterpret_cast<uint4*>(alo + off) = lo;
+                    uint32_t h0, l0, h1, l1;
+                    split2(x.x, x.y, h0, l0);
+                    split2(x.z, x.w, h1, l1);
+                    // Lane pairs hold 8 consecutive elements: the even lane assembles the hi chunk,
+                    // the odd lane the lo chunk.
+                    const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
+                    const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
+                    const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
+                    if (!odd) *reinterpret_cast<uint4*>(ahi + off) = pack4(h0, h1, got0, got1);
+                    else *reinterpret_cast<uint4*>(alo + off) = pack4(got0, got1, l0, l1);
                 }
                 fence_proxy_async();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&conv[s]);
-                if (++s == S) { s = 0; ph ^= 1; }
+                if (lane == 0) {
+                    mbar_arrive(&f_empty[fs]);
+                    mbar_arrive(&o_full[os]);
+                }
+                if (++fs == FS) { fs = 0; fph ^= 1; }
+                if (++os == OS) { os = 0; oph ^= 1; }
+            }
+        }
+        if (b_issuer) {
+            for (int i = 0; i < OS; ++i) {
+                if (b_issued[i] < 0) continue;
+                const unsigned long long t0 = gtimer();
+                while (!mbar_try(&b_full[i], (uint32_t)b_issued[i]) && gtimer() - t0 < kTimeoutNs) {}
             }
         }
     } else {
         // ------------------------------------------------------------- epilogue
         const int q4 = warp & 3;                 // TMEM lane quarter this warp may access
+        const int ew = warp - (2 + kConvWarps);  // 0..3
         const int row = q4 * 32 + lane;          // accumulator row = MMA M index
+        uint8_t* stage0 = epi + (size_t)ew * 2 * kEpiBuf;
+        int sb = 0;
         int ab = 0;
         uint32_t aph = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
             if (!mbar_wait(&acc_full[ab], aph, abort_flag)) break;
             tc_fence_after();
             const int64_t jb = t / P.tiles_m, mt = t - jb * P.tiles_m;
-            int64_t cbase;
-            bool rvalid;
+            int64_t k, r0;            // slice and first row (i for GEOM_MN, k for GEOM_K) of this warp
             if (GEOM == GEOM_MN) {
-                const int64_t mper = (P.inner + kBM - 1) / kBM;
-                const int64_t k = mt / mper, i = (mt - k * mper) * kBM + row;
-                rvalid = i < P.inner;
-                cbase = k * P.m * P.inner + i;
+                k = mt / mper;
+                r0 = (mt - k * mper) * kBM + q4 * 32;
             } else {
-                const int64_t k = mt * kBM + row;
-                rvalid = k < P.outer;
-                cbase = k * P.m;
+                k = 0;
+                r0 = mt * kBM + q4 * 32;
             }
+            const int64_t jrem = P.m - (int64_t)jb * P.nt;
+            const int jleft = jrem < P.nt ? (int)jrem : P.nt;
             const uint32_t tbase = tmem_base + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(ab * P.nt);
             for (int cc = 0; cc < P.nt; cc += 32) {
                 uint32_t v[32];
                 tmem_ld32(tbase + (uint32_t)cc, v);
-                const int64_t j0 = (int64_t)jb * P.nt + cc;
-                if (rvalid) {
+                if (cc >= jleft) continue;
+                const int j0 = jb * P.nt + cc;
+                if (P.tma_c) {
+                    // Stage a 32 x 32 block in shared memory and store it with one TMA copy.
+                    uint8_t* buf = stage0 + sb * kEpiBuf;
+                    if (lane == 0) bulk_wait_read1();      // the copy that last read `buf` has finished reading
+                    __syncwarp();
                     if (GEOM == GEOM_MN) {
+                        // smem [32 j][32 i]: this lane owns column i = lane
+                        float* b32 = reinterpret_cast<float*>(buf);
 #pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            const int64_t j = j0 + c;
-                            if (j < P.m) P.c[cbase + j * P.inner] = __uint_as_float(v[c]);
-                        }
-                    } else if (P.vec_c && j0 + 32 <= P.m) {
-                        float4* dst = reinterpret_cast<float4*>(P.c + cbase + j0);
+                        for (int c = 0; c < 32; ++c) b32[c * 32 + lane] = __uint_as_float(v[c]);
+                    } else {
+                        // smem [32 k][32 j] with the 128-byte swizzle: this lane owns row k = lane
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
-                            dst[c] = make_float4(__uint_as_float(v[4 * c]), __uint_as_float(v[4 * c + 1]),
-                                                 __uint_as_float(v[4 * c + 2]), __uint_as_float(v[4 * c + 3]));
-                    } else {
+                            *reinterpret_cast<uint4*>(buf + lane * 128 + ((c ^ (lane & 7)) << 4)) =
+                                make_uint4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                    }
+                    fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0) {
+                        if (GEOM == GEOM_MN) tma_store_3d(&cmap, buf, (int)r0, j0, (int)k);
+                        else tma_store_2d(&cmap, buf, j0, (int)r0);
+                        bulk_commit();
+                    }
+                    sb ^= 1;
+                } else {
+                    // Direct stores (C rows not 16-byte aligned for a tensor map).
+                    const int64_t r = r0 + lane;
+                    const bool rvalid = GEOM == GEOM_MN ? r < P.inner : r < P.outer;
+                    if (rvalid) {
+                        float* p = GEOM == GEOM_MN ? P.c + (k * P.m + j0) * P.inner + r : P.c + r * P.m + j0;
+                        const int64_t cs = GEOM == GEOM_MN ? P.inner : 1;
 #pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            const int64_t j = j0 + c;
-                            if (j < P.m) P.c[cbase + j] = __uint_as_float(v[c]);
-                        }
+                        for (int c = 0; c < 32; ++c)
+                            if (cc + c < jleft) p[(int64_t)c * cs] = __uint_as_float(v[c]);
                     }
                 }
             }
@@ -459,6 +546,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_bf16x3_kernel(const __grid_con
             if (lane == 0) mbar_arrive(&acc_empty[ab]);
             if (++ab == 2) { ab = 0; aph ^= 1; }
         }
+        if (lane == 0) bulk_wait_all();   // every TMA store of this warp has completed
+        (void)row;
     }
 
     tc_fence_before();
@@ -471,15 +560,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_bf16x3_kernel(const __grid_con
 }
 
 // B (m x nq, column- or row-major FP32) -> bf16 hi/lo images, one per (j block, K chunk),
-// each NT rows x 32 l in the K-major SW64 layout the MMA reads. Zero outside B.
+// each NT rows x 16 l in the K-major SW32 layout the MMA reads. Zero outside B.
 __global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m, int64_t nq, int nt, int jblocks,
                                int kchunks, uint8_t* __restrict__ img)
 {
-    const int64_t total = (int64_t)jblocks * kchunks * nt * 4;     // 4 chunks of 8 l per row
-    const uint32_t part_bytes = (uint32_t)nt * 64u;
+    const int64_t total = (int64_t)jblocks * kchunks * nt * 2;     // 2 chunks of 8 l per row
+    const uint32_t part_bytes = (uint32_t)nt * (kBK * 2);
     for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(u & 3);
-        const int64_t rrow = u >> 2;
+        const int c = (int)(u & 1);
+        const int64_t rrow = u >> 1;
         const int jl = (int)(rrow % nt);
         const int64_t bk = rrow / nt;
         const int kc = (int)(bk % kchunks);
@@ -497,7 +586,7 @@ __global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m,
         split2(x[4], x[5], h.z, lo.z);
         split2(x[6], x[7], h.w, lo.w);
         uint8_t* base = img + (size_t)((int64_t)jb * kchunks + kc) * 2 * part_bytes;
-        const uint32_t off = kmaj_sw64_off((uint32_t)jl, (uint32_t)c);
+        const uint32_t off = kmaj_sw32_off((uint32_t)jl, (uint32_t)c);
         *reinterpret_cast<uint4*>(base + off) = h;
         *reinterpret_cast<uint4*>(base + part_bytes + off) = lo;
     }
@@ -577,8 +666,37 @@ bool encode_a_map(const View3& v, int geom, CUtensorMap* map)
         cuuint32_t box[2] = {kBK, kBM};
         cuuint32_t es[2] = {1, 1};
         r = cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(v.a), dims, strides, box,
-                                   es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+    return r == CUDA_SUCCESS;
+}
+
+// C as a tensor map for the TMA-store epilogue: 32 x 32 boxes. False when C's rows are not
+// 16-byte aligned (the epilogue then stores directly).
+bool encode_c_map(const View3& v, int geom, CUtensorMap* map)
+{
+    EncodeTiledFn cuTensorMapEncodeTiled = encode_fn();
+    if (!cuTensorMapEncodeTiled) return false;
+    if ((reinterpret_cast<uintptr_t>(v.c) & 15u) != 0) return false;
+    CUresult r;
+    if (geom == GEOM_MN) {
+        cuuint64_t dims[3] = {(cuuint64_t)v.inner, (cuuint64_t)v.m, (cuuint64_t)v.outer};
+        cuuint64_t strides[2] = {(cuuint64_t)v.inner * 4, (cuuint64_t)v.inner * v.m * 4};
+        cuuint32_t box[3] = {32, 32, 1};
+        cuuint32_t es[3] = {1, 1, 1};
+        r = cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, v.c, dims, strides, box, es,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    } else {
+        if (v.m % 4 != 0) return false;
+        cuuint64_t dims[2] = {(cuuint64_t)v.m, (cuuint64_t)v.outer};
+        cuuint64_t strides[1] = {(cuuint64_t)v.m * 4};
+        cuuint32_t box[2] = {32, 32};
+        cuuint32_t es[2] = {1, 1};
+        r = cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, v.c, dims, strides, box, es,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     }
     return r == CUDA_SUCCESS;
 }
@@ -587,6 +705,50 @@ int geometry_of(const View3& v)
 {
     if (v.inner == 1) return (v.nq % 4 == 0) ? GEOM_K : -1;
     return (v.inner % 4 == 0) ? GEOM_MN : -1;
+}
+
+// Splits B into `img` (tc_image_bytes(v) bytes) and launches the bf16x3 kernel for v on stream s.
+cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaStream_t s)
+{
+    const int geom = geometry_of(v);
+    const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
+    const int jblocks = (int)((v.m + nt - 1) / nt);
+    const int kchunks = (int)((v.nq + kBK - 1) / kBK);
+    CUtensorMap amap, cmap;
+    if (!encode_a_map(v, geom, &amap)) return cudaErrorInvalidValue;
+    TcParams P{};
+    P.tma_c = encode_c_map(v, geom, &cmap) ? 1 : 0;
+    if (!P.tma_c) std::memset(&cmap, 0, sizeof(cmap));
+    P.c = static_cast<float*>(v.c);
+    P.bimg = img;
+    P.status = status;
+    P.outer = v.outer;
+    P.nq = v.nq;
+    P.inner = v.inner;
+    P.m = v.m;
+    P.tiles_m = geom == GEOM_MN ? v.outer * ((v.inner + kBM - 1) / kBM) : (v.outer + kBM - 1) / kBM;
+    P.tiles = P.tiles_m * jblocks;
+    P.nt = nt;
+    P.jblocks = jblocks;
+    P.kchunks = kchunks;
+    size_t smem = 0;
+    if (!choose_stages(nt, P.fstages, P.ostages, smem)) return cudaErrorNotSupported;
+
+    const int64_t total = (int64_t)jblocks * kchunks * nt * 2;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
+    split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks, kchunks,
+                                          img);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int grid = (int)std::min<int64_t>(P.tiles, sms);
+    if (geom == GEOM_MN) {
+        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_MN><<<grid, kThreads, smem, s>>>(amap, cmap, P);
+    } else {
+        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_K><<<grid, kThreads, smem, s>>>(amap, cmap, P);
+    }
+    return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
 }  // namespace
@@ -615,69 +777,11 @@ cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid)
         e = cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
     }
-    const int geom = geometry_of(v);
-    const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
-    const int jblocks = (int)((v.m + nt - 1) / nt);
-    const int kchunks = (int)((v.nq + kBK - 1) / kBK);
-    const SmemLayout L = smem_layout(nt);
-    const size_t img_bytes = (size_t)jblocks * kchunks * 2 * L.b_bytes;
-
     DevState* st = nullptr;
     if ((e = state_for(dev, st)) != cudaSuccess) return e;
     void* img = nullptr;
-    if ((e = cudaMallocAsync(&img, img_bytes, s)) != cudaSuccess) return e;
-
-    CUtensorMap amap;
-    if (!encode_a_map(v, geom, &amap)) {
-        cudaFreeAsync(img, s);
-        return cudaErrorInvalidValue;
-    }
-
-    TcParams P{};
-    P.c = static_cast<float*>(v.c);
-    P.bimg = static_cast<const uint8_t*>(img);
-    P.status = st->status;
-    P.outer = v.outer;
-    P.nq = v.nq;
-    P.inner = v.inner;
-    P.m = v.m;
-    P.tiles_m = geom == GEOM_MN ? v.outer * ((v.inner + kBM - 1) / kBM) : (v.outer + kBM - 1) / kBM;
-    P.tiles = P.tiles_m * jblocks;
-    P.nt = nt;
-    P.jblocks = jblocks;
-    P.kchunks = kchunks;
-    P.vec_c = (geom == GEOM_K) && (v.m % 4 == 0) && ((reinterpret_cast<uintptr_t>(v.c) & 15u) == 0);
-    const size_t ctrl = 1024;
-    const size_t budget = 227 * 1024 - 1024 - ctrl;
-    int stages = (int)(budget / L.stage_bytes);
-    if (stages > kMaxStages) stages = kMaxStages;
-    if (stages < 2) {
-        cudaFreeAsync(img, s);
-        return cudaErrorNotSupported;
-    }
-    P.stages = stages;
-    const size_t smem = 1024 + (size_t)stages * L.stage_bytes + ctrl;
-
-    // split B once per call
-    {
-        const int64_t total = (int64_t)jblocks * kchunks * nt * 4;
-        const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-        split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks,
-                                              kchunks, static_cast<uint8_t*>(img));
-        if ((e = cudaGetLastError()) != cudaSuccess) {
-            cudaFreeAsync(img, s);
-            return e;
-        }
-    }
-    const int grid = (int)std::min<int64_t>(P.tiles, g_sm_count);
-    if (geom == GEOM_MN) {
-        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_MN><<<grid, kThreads, smem, s>>>(amap, P);
-    } else {
-        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_K><<<grid, kThreads, smem, s>>>(amap, P);
-    }
-    if (e == cudaSuccess) e = cudaGetLastError();
+    if ((e = cudaMallocAsync(&img, tc_image_bytes(v), s)) != cudaSuccess) return e;
+    e = run_bf16x3(v, static_cast<uint8_t*>(img), st->status, g_sm_count, s);
     cudaFreeAsync(img, s);
     return e;
 }
@@ -746,52 +850,8 @@ cudaError_t launch_tc_noalloc(const View3& v, cudaStream_t s, int* kid)
     if ((e = noalloc_symbols(dev, sy)) != cudaSuccess) return e;
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-
-    const int geom = geometry_of(v);
-    const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
-    const int jblocks = (int)((v.m + nt - 1) / nt);
-    const int kchunks = (int)((v.nq + kBK - 1) / kBK);
-    const SmemLayout L = smem_layout(nt);
-
-    CUtensorMap amap;
-    if (!encode_a_map(v, geom, &amap)) return cudaErrorInvalidValue;
     if ((e = cudaMemsetAsync(sy.status, 0, sizeof(int), s)) != cudaSuccess) return e;
-
-    TcParams P{};
-    P.c = static_cast<float*>(v.c);
-    P.bimg = sy.image;
-    P.status = sy.status;
-    P.outer = v.outer;
-    P.nq = v.nq;
-    P.inner = v.inner;
-    P.m = v.m;
-    P.tiles_m = geom == GEOM_MN ? v.outer * ((v.inner + kBM - 1) / kBM) : (v.outer + kBM - 1) / kBM;
-    P.tiles = P.tiles_m * jblocks;
-    P.nt = nt;
-    P.jblocks = jblocks;
-    P.kchunks = kchunks;
-    P.vec_c = (geom == GEOM_K) && (v.m % 4 == 0) && ((reinterpret_cast<uintptr_t>(v.c) & 15u) == 0);
-    const size_t ctrl = 1024;
-    int stages = (int)((227 * 1024 - 1024 - ctrl) / L.stage_bytes);
-    if (stages > kMaxStages) stages = kMaxStages;
-    if (stages < 2) return cudaErrorNotSupported;
-    P.stages = stages;
-    const size_t smem = 1024 + (size_t)stages * L.stage_bytes + ctrl;
-
-    const int64_t total = (int64_t)jblocks * kchunks * nt * 4;
-    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-    split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks, kchunks,
-                                          sy.image);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    const int grid = (int)std::min<int64_t>(P.tiles, sms);
-    if (geom == GEOM_MN) {
-        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_MN><<<grid, kThreads, smem, s>>>(amap, P);
-    } else {
-        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_K><<<grid, kThreads, smem, s>>>(amap, P);
-    }
-    return e == cudaSuccess ? cudaGetLastError() : e;
+    return run_bf16x3(v, sy.image, sy.status, sms, s);
 }
 
 int tc_read_status()

@@ -19,7 +19,7 @@ void tc_release_buffers();
 int tc_read_status();
 
 // Largest pre-split B image the allocation-free bf16x3 variant can hold (bytes):
-// ceil(m/16)*16 * ceil(n_q/32)*32 * 4 <= 1 MiB for m <= 256, e.g. m = 256 with n_q <= 1024.
+// ceil(m/16)*16 * ceil(n_q/16)*16 * 4 <= 1 MiB for m <= 256, e.g. m = 256 with n_q <= 1024.
 constexpr size_t kNoAllocImageBytes = size_t(1) << 20;
 
 // Bytes of the pre-split B image a bf16x3 launch of this view needs.
