@@ -38,7 +38,9 @@ namespace tlibttm {
 namespace {
 
 constexpr int kConvWarps = 8;                   // converter warps
-constexpr int kThreads = (2 + kConvWarps + 4) * 32;  // producer, MMA, converters, 4 epilogue warps
+constexpr int kConvGroups = 4;                  // groups converting different stages at the same time
+constexpr int kGroupWarps = kConvWarps / kConvGroups;
+constexpr int kThreads = (3 + kConvWarps + 4) * 32;  // A producer, MMA, B producer, converters, 4 epilogue warps
 constexpr int kConvThreads = kConvWarps * 32;
 constexpr int kBM = 128;       // MMA M
 constexpr int kBK = 16;        // l per stage (one MMA K step)
@@ -229,47 +231,54 @@ struct TcParams {
     int nt;                  // MMA N (multiple of 16, <= 256)
     int jblocks;
     int kchunks;
-    int fstages;             // FP32 staging ring depth
-    int ostages;             // bf16 operand ring depth
+    int fstages;             // A ring depth (FP32 tile, converted in place)
+    int ostages;             // B ring depth
     int tma_c;               // epilogue stores C through the C tensor map
 };
 
-// Shared memory: [FP32 ring][operand ring: (A_hi, A_lo, B_hi, B_lo) per stage][epilogue staging][barriers].
+// Shared memory: [A ring: FP32 tile, converted in place to bf16 hi|lo][B ring: B_hi|B_lo]
+//                [epilogue staging][barriers].
 struct SmemLayout {
-    uint32_t f32_bytes, abf_bytes, b_bytes, op_bytes;
+    uint32_t a_bytes, abf_bytes, b_bytes, bstage_bytes;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int nt)
 {
     SmemLayout L;
-    L.f32_bytes = kBM * kBK * 4;            // 8 KB
-    L.abf_bytes = kBM * kBK * 2;            // 4 KB per part
+    L.a_bytes = kBM * kBK * 4;              // 8 KB FP32 tile (its bf16 hi and lo halves after conversion)
+    L.abf_bytes = kBM * kBK * 2;            // 4 KB per bf16 part
     L.b_bytes = (uint32_t)nt * kBK * 2;     // per part, multiple of 512
-    L.op_bytes = 2 * L.abf_bytes + 2 * L.b_bytes;
+    L.bstage_bytes = 2 * L.b_bytes;
     return L;
 }
 
-constexpr int kMaxF = 16, kMaxO = 4;
+constexpr int kMaxA = 24, kMaxB = 4;
 constexpr uint32_t kEpiBuf = 32 * 32 * 4;        // one 32 x 32 fp32 staging tile
 constexpr uint32_t kEpiBytes = 4 * 2 * kEpiBuf;  // 4 epilogue warps, double-buffered
 constexpr size_t kCtrlBytes = 1024;
 constexpr size_t kSmemBudget = 227 * 1024;
 
 // Ring depths for a given N tile; false if the minimum does not fit.
-__host__ inline bool choose_stages(int nt, int& fs, int& os, size_t& smem)
+__host__ inline bool choose_stages(int nt, int& as, int& bs, size_t& smem)
 {
     const SmemLayout L = smem_layout(nt);
     const size_t avail = kSmemBudget - 1024 - kCtrlBytes - kEpiBytes;
-    os = kMaxO;
-    while (os > 2 && (size_t)os * L.op_bytes + 6 * L.f32_bytes > avail) --os;
-    if ((size_t)os * L.op_bytes + 6 * L.f32_bytes > avail) return false;
-    fs = (int)((avail - (size_t)os * L.op_bytes) / L.f32_bytes);
-    if (fs > kMaxF) fs = kMaxF;
-    smem = 1024 + (size_t)fs * L.f32_bytes + (size_t)os * L.op_bytes + kEpiBytes + kCtrlBytes;
+    bs = kMaxB;
+    while (bs > 2 && (size_t)bs * L.bstage_bytes + 8 * L.a_bytes > avail) --bs;
+    if ((size_t)bs * L.bstage_bytes + 8 * L.a_bytes > avail) return false;
+    as = (int)((avail - (size_t)bs * L.bstage_bytes) / L.a_bytes);
+    if (as > kMaxA) as = kMaxA;
+    smem = 1024 + (size_t)as * L.a_bytes + (size_t)bs * L.bstage_bytes + kEpiBytes + kCtrlBytes;
     return true;
 }
 
 __device__ __forceinline__ uint4 pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) { return make_uint4(a, b, c, d); }
+
+// Named barrier of one converter group (ids 1..kConvGroups; id 0 is __syncthreads).
+__device__ __forceinline__ void conv_barrier(int g)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "n"(kGroupWarps * 32) : "memory");
+}
 
 template <int GEOM>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -278,38 +287,36 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const SmemLayout L = smem_layout(P.nt);
-    const int FS = P.fstages, OS = P.ostages;
-    uint8_t* fring = smem;
-    uint8_t* oring = smem + (size_t)FS * L.f32_bytes;
-    uint8_t* epi = oring + (size_t)OS * L.op_bytes;
+    const int AS = P.fstages, BS = P.ostages;
+    uint8_t* aring = smem;
+    uint8_t* bring = smem + (size_t)AS * L.a_bytes;
+    uint8_t* epi = bring + (size_t)BS * L.bstage_bytes;
     uint8_t* ctrl = epi + kEpiBytes;
-    uint64_t* f_full = reinterpret_cast<uint64_t*>(ctrl);   // [FS]  TMA of A landed
-    uint64_t* f_empty = f_full + kMaxF;                       // [FS]  converters done reading
-    uint64_t* b_full = f_empty + kMaxF;                       // [OS]  B image landed
-    uint64_t* o_full = b_full + kMaxO;                        // [OS]  converted A written
-    uint64_t* o_empty = o_full + kMaxO;                       // [OS]  MMAs done reading
-    uint64_t* acc_full = o_empty + kMaxO;                     // [2]
+    uint64_t* a_full = reinterpret_cast<uint64_t*>(ctrl);   // [AS]  TMA of the FP32 tile landed
+    uint64_t* a_conv = a_full + kMaxA;                        // [AS]  bf16 hi/lo written in place
+    uint64_t* a_empty = a_conv + kMaxA;                       // [AS]  MMAs done reading
+    uint64_t* b_full = a_empty + kMaxA;                       // [BS]  B image landed
+    uint64_t* b_empty = b_full + kMaxB;                       // [BS]  MMAs done reading
+    uint64_t* acc_full = b_empty + kMaxB;                     // [2]
     uint64_t* acc_empty = acc_full + 2;                       // [2]
     uint64_t* drain = acc_empty + 2;                          // [1]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    auto f32_at = [&](int s) { return fring + (size_t)s * L.f32_bytes; };
-    auto ahi_at = [&](int s) { return oring + (size_t)s * L.op_bytes; };
-    auto alo_at = [&](int s) { return ahi_at(s) + L.abf_bytes; };
-    auto bhi_at = [&](int s) { return alo_at(s) + L.abf_bytes; };
+    auto a_at = [&](int s) { return aring + (size_t)s * L.a_bytes; };
+    auto bhi_at = [&](int s) { return bring + (size_t)s * L.bstage_bytes; };
     auto blo_at = [&](int s) { return bhi_at(s) + L.b_bytes; };
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < FS; ++s) {
-            mbar_init(&f_full[s], 1);
-            mbar_init(&f_empty[s], kConvWarps);
+        for (int s = 0; s < AS; ++s) {
+            mbar_init(&a_full[s], 1);
+            mbar_init(&a_conv[s], kGroupWarps);
+            mbar_init(&a_empty[s], 1);
         }
-        for (int s = 0; s < OS; ++s) {
+        for (int s = 0; s < BS; ++s) {
             mbar_init(&b_full[s], 1);
-            mbar_init(&o_full[s], kConvWarps);
-            mbar_init(&o_empty[s], 1);
+            mbar_init(&b_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(&acc_full[b], 1);
@@ -339,146 +346,164 @@ __global__ void __launch_bounds__(kThreads, 1)
             int s = 0;
             uint32_t ph = 0;
             bool ok = true;
-            int issued[kMaxF];
-            for (int i = 0; i < kMaxF; ++i) issued[i] = -1;
+            int issued[kMaxA];
+            for (int i = 0; i < kMaxA; ++i) issued[i] = -1;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 const int64_t mt = t % P.tiles_m;
                 for (int kc = 0; kc < kchunks; ++kc) {
-                    if (!mbar_wait(&f_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(&a_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&f_full[s], L.f32_bytes);
+                    mbar_expect_tx(&a_full[s], L.a_bytes);
                     if (GEOM == GEOM_MN) {
                         const int64_t k = mt / mper, ib = mt - k * mper;
-                        tma_load_3d(f32_at(s), &amap, &f_full[s], (int)(ib * kBM), kc * kBK, (int)k);
+                        tma_load_3d(a_at(s), &amap, &a_full[s], (int)(ib * kBM), kc * kBK, (int)k);
                     } else {
-                        tma_load_2d(f32_at(s), &amap, &f_full[s], kc * kBK, (int)(mt * kBM));
+                        tma_load_2d(a_at(s), &amap, &a_full[s], kc * kBK, (int)(mt * kBM));
                     }
-                    if (++s == FS) { s = 0; ph ^= 1; }
+                    if (++s == AS) { s = 0; ph ^= 1; }
                 }
             }
             // None of this CTA's bulk copies may still be in flight when it exits.
-            for (int i = 0; i < FS; ++i) {
+            for (int i = 0; i < AS; ++i) {
                 if (issued[i] < 0) continue;
                 const unsigned long long t0 = gtimer();
-                while (!mbar_try(&f_full[i], (uint32_t)issued[i]) && gtimer() - t0 < kTimeoutNs) {}
+                while (!mbar_try(&a_full[i], (uint32_t)issued[i]) && gtimer() - t0 < kTimeoutNs) {}
+            }
+        }
+    } else if (warp == 2) {
+        // ------------------------------------------------------------- B producer (bulk copies)
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            int issued[kMaxB];
+            for (int i = 0; i < kMaxB; ++i) issued[i] = -1;
+            for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                const int64_t jb = t / P.tiles_m;
+                for (int kc = 0; kc < kchunks; ++kc) {
+                    if (!mbar_wait(&b_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    issued[s] = (int)ph;
+                    mbar_expect_tx(&b_full[s], 2 * L.b_bytes);
+                    const uint8_t* img = P.bimg + ((size_t)(jb * kchunks + kc) * 2) * L.b_bytes;
+                    bulk_load(bhi_at(s), img, L.b_bytes, &b_full[s]);
+                    bulk_load(blo_at(s), img + L.b_bytes, L.b_bytes, &b_full[s]);
+                    if (++s == BS) { s = 0; ph ^= 1; }
+                }
+            }
+            for (int i = 0; i < BS; ++i) {
+                if (issued[i] < 0) continue;
+                const unsigned long long t0 = gtimer();
+                while (!mbar_try(&b_full[i], (uint32_t)issued[i]) && gtimer() - t0 < kTimeoutNs) {}
             }
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = idesc_bf16(P.nt, GEOM == GEOM_MN);
-            int s = 0;
-            uint32_t ph = 0;
+            int as = 0, bs = 0;
+            uint32_t aph = 0, bph = 0;
             int ab = 0;
-            uint32_t aph = 0;
+            uint32_t cph = 0;
             bool ok = true;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                if (!mbar_wait(&acc_empty[ab], aph ^ 1, abort_flag)) break;
+                if (!mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag)) break;
                 tc_fence_after();
                 const uint32_t dcol = tmem_base + (uint32_t)(ab * P.nt);
                 for (int kc = 0; kc < kchunks; ++kc) {
-                    if (!mbar_wait(&b_full[s], ph, abort_flag) || !mbar_wait(&o_full[s], ph, abort_flag)) {
+                    if (!mbar_wait(&b_full[bs], bph, abort_flag) || !mbar_wait(&a_conv[as], aph, abort_flag)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
+                    const uint32_t ahi = su32(a_at(as)), alo = ahi + L.abf_bytes;
                     uint64_t dahi, dalo;
                     if (GEOM == GEOM_MN) {
-                        dahi = smem_desc(su32(ahi_at(s)), 1024u, 2048u, kLayoutSW128);
-                        dalo = smem_desc(su32(alo_at(s)), 1024u, 2048u, kLayoutSW128);
+                        dahi = smem_desc(ahi, 1024u, 2048u, kLayoutSW128);
+                        dalo = smem_desc(alo, 1024u, 2048u, kLayoutSW128);
                     } else {
-                        dahi = smem_desc(su32(ahi_at(s)), 16u, 256u, kLayoutSW32);
-                        dalo = smem_desc(su32(alo_at(s)), 16u, 256u, kLayoutSW32);
+                        dahi = smem_desc(ahi, 16u, 256u, kLayoutSW32);
+                        dalo = smem_desc(alo, 16u, 256u, kLayoutSW32);
                     }
-                    const uint64_t dbhi = smem_desc(su32(bhi_at(s)), 16u, 256u, kLayoutSW32);
-                    const uint64_t dblo = smem_desc(su32(blo_at(s)), 16u, 256u, kLayoutSW32);
+                    const uint64_t dbhi = smem_desc(su32(bhi_at(bs)), 16u, 256u, kLayoutSW32);
+                    const uint64_t dblo = smem_desc(su32(blo_at(bs)), 16u, 256u, kLayoutSW32);
                     mma_bf16(dcol, dahi, dbhi, idesc, kc == 0 ? 0u : 1u);
                     mma_bf16(dcol, dahi, dblo, idesc, 1u);
                     mma_bf16(dcol, dalo, dbhi, idesc, 1u);
-                    mma_commit(&o_empty[s]);   // operand stage free once these MMAs have read it
-                    if (++s == OS) { s = 0; ph ^= 1; }
+                    mma_commit(&a_empty[as]);   // stages free once these MMAs have read them
+                    mma_commit(&b_empty[bs]);
+                    if (++as == AS) { as = 0; aph ^= 1; }
+                    if (++bs == BS) { bs = 0; bph ^= 1; }
                 }
                 if (!ok) break;
                 mma_commit(&acc_full[ab]);     // accumulator ready for the epilogue
-                if (++ab == 2) { ab = 0; aph ^= 1; }
+                if (++ab == 2) { ab = 0; cph ^= 1; }
             }
             // No MMA of this CTA may still be writing TMEM when it is freed.
             mma_commit(drain);
             const unsigned long long t0 = gtimer();
             while (!mbar_try(drain, 0) && gtimer() - t0 < kTimeoutNs) {}
         }
-    } else if (warp < 2 + kConvWarps) {
-        // ------------------------------------------------------------- converters (+ B loads)
-        const int ct = threadIdx.x - 64;   // 0 .. kConvThreads-1
-        const bool b_issuer = ct == 0;
+    } else if (warp < 3 + kConvWarps) {
+        // ------------------------------------------------------------- converters (in place)
+        // kConvGroups groups of kGroupWarps warps; group g converts the stages with sequence number
+        // n, n % kConvGroups == g, so that many tiles are converted at once.
+        const int g = (warp - 3) / kGroupWarps;
+        const int gt = threadIdx.x - 96 - g * kGroupWarps * 32;   // 0 .. kGroupWarps*32-1
         const bool odd = lane & 1;
-        int fs = 0, os = 0;
-        uint32_t fph = 0, oph = 0;
+        constexpr int kIters = (kBM * kBK / 4) / (kGroupWarps * 32);
         bool ok = true;
-        int b_issued[kMaxO];
-        for (int i = 0; i < kMaxO; ++i) b_issued[i] = -1;
-        for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-            const int64_t jb = t / P.tiles_m;
-            for (int kc = 0; kc < kchunks; ++kc) {
-                if (!mbar_wait(&o_empty[os], oph ^ 1, abort_flag)) { ok = false; break; }
-                if (b_issuer) {
-                    b_issued[os] = (int)oph;
-                    mbar_expect_tx(&b_full[os], 2 * L.b_bytes);
-                    const uint8_t* img = P.bimg + ((size_t)(jb * kchunks + kc) * 2) * L.b_bytes;
-                    bulk_load(bhi_at(os), img, L.b_bytes, &b_full[os]);
-                    bulk_load(blo_at(os), img + L.b_bytes, L.b_bytes, &b_full[os]);
-                }
-                if (!mbar_wait(&f_full[fs], fph, abort_flag)) { ok = false; break; }
-                const uint8_t* f = f32_at(fs);
-                uint8_t* ahi = ahi_at(os);
-                uint8_t* alo = alo_at(os);
+        int64_t n = 0;   // sequence number of the chunk across this CTA's tiles
+        // Every thread of a group runs every iteration of its parity and reaches the group barrier
+        // the same number of times; once the CTA aborts, the waits are skipped and no work is done.
+        for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+            for (int kc = 0; kc < kchunks; ++kc, ++n) {
+                if ((int)(n % kConvGroups) != g) continue;
+                const int s = (int)(n % AS);
+                const uint32_t ph = (uint32_t)((n / AS) & 1);
+                const bool got = ok && mbar_wait(&a_full[s], ph, abort_flag);
+                const bool have = __all_sync(0xffffffffu, got);
+                if (!have) ok = false;
+                uint8_t* buf = a_at(s);
+                float4 x[kIters];
+                uint32_t off[kIters];
 #pragma unroll
-                for (int it = 0; it < (kBM * kBK / 4) / kConvThreads; ++it) {
-                    const int v = ct + kConvThreads * it;   // float4 index within the 8 KB tile
-                    float4 x;
-                    uint32_t off;
+                for (int it = 0; it < kIters; ++it) {
+                    const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
                     if (GEOM == GEOM_MN) {
                         const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
-                        x = *reinterpret_cast<const float4*>(f + l * 512 + w * 16);
-                        off = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
+                        if (have) x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
+                        off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
                     } else {
                         const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
-                        x = *reinterpret_cast<const float4*>(f + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
-                        off = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
+                        if (have) x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                        off[it] = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
                     }
-                    uint32_t h0, l0, h1, l1;
-                    split2(x.x, x.y, h0, l0);
-                    split2(x.z, x.w, h1, l1);
-                    // Lane pairs hold 8 consecutive elements: the even lane assembles the hi chunk,
-                    // the odd lane the lo chunk.
-                    const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
-                    const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
-                    const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
-                    if (!odd) *reinterpret_cast<uint4*>(ahi + off) = pack4(h0, h1, got0, got1);
-                    else *reinterpret_cast<uint4*>(alo + off) = pack4(got0, got1, l0, l1);
                 }
-                fence_proxy_async();
-                __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(&f_empty[fs]);
-                    mbar_arrive(&o_full[os]);
+                conv_barrier(g);   // the whole FP32 tile is in registers before it is overwritten
+                if (have) {
+#pragma unroll
+                    for (int it = 0; it < kIters; ++it) {
+                        uint32_t h0, l0, h1, l1;
+                        split2(x[it].x, x[it].y, h0, l0);
+                        split2(x[it].z, x[it].w, h1, l1);
+                        // Lane pairs hold 8 consecutive elements: the even lane assembles the hi
+                        // chunk, the odd lane the lo chunk.
+                        const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
+                        const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
+                        const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
+                        if (!odd) *reinterpret_cast<uint4*>(buf + off[it]) = pack4(h0, h1, got0, got1);
+                        else *reinterpret_cast<uint4*>(buf + L.abf_bytes + off[it]) = pack4(got0, got1, l0, l1);
+                    }
+                    fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&a_conv[s]);
                 }
-                if (++fs == FS) { fs = 0; fph ^= 1; }
-                if (++os == OS) { os = 0; oph ^= 1; }
-            }
-        }
-        if (b_issuer) {
-            for (int i = 0; i < OS; ++i) {
-                if (b_issued[i] < 0) continue;
-                const unsigned long long t0 = gtimer();
-                while (!mbar_try(&b_full[i], (uint32_t)b_issued[i]) && gtimer() - t0 < kTimeoutNs) {}
             }
         }
     } else {
         // ------------------------------------------------------------- epilogue
         const int q4 = warp & 3;                 // TMEM lane quarter this warp may access
-        const int ew = warp - (2 + kConvWarps);  // 0..3
-        const int row = q4 * 32 + lane;          // accumulator row = MMA M index
+        const int ew = warp - (3 + kConvWarps);  // 0..3
         uint8_t* stage0 = epi + (size_t)ew * 2 * kEpiBuf;
         int sb = 0;
         int ab = 0;
@@ -506,7 +531,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (P.tma_c) {
                     // Stage a 32 x 32 block in shared memory and store it with one TMA copy.
                     uint8_t* buf = stage0 + sb * kEpiBuf;
-                    if (lane == 0) bulk_wait_read1();      // the copy that last read `buf` has finished reading
+                    if (lane == 0) bulk_wait_read1();      // the copy that last read `buf` has finished reading it
                     __syncwarp();
                     if (GEOM == GEOM_MN) {
                         // smem [32 j][32 i]: this lane owns column i = lane
@@ -547,7 +572,6 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (++ab == 2) { ab = 0; aph ^= 1; }
         }
         if (lane == 0) bulk_wait_all();   // every TMA store of this warp has completed
-        (void)row;
     }
 
     tc_fence_before();
