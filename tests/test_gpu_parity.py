@@ -242,3 +242,33 @@ def test_ttmpy_torch_and_permuted_views(cuda):
     A32 = A.astype(np.float32)
     assert np.allclose(tp.ttm(2, A32, B.astype(np.float32)), np.einsum("ijk,xj->ixk", A32, B), rtol=1e-5,
                        atol=1e-5)
+
+
+@pytest.mark.parametrize("dtype,prec", [(np.float32, _lib.PREC_PLAIN), (np.float32, _lib.PREC_BF16X3),
+                                        (np.float64, _lib.PREC_PLAIN)])
+@pytest.mark.parametrize("q", [1, 2, 3])
+def test_pipelined_host_staging(cuda, dtype, prec, q):
+    """Large host operands go through the chunked, overlapped copy-in / compute / copy-out path
+    (chunks of whole slices when there are many, column blocks of each slice when there are few)."""
+    import torch
+    na, pia = [256, 256, 320], [1, 2, 3]    # 84 MB fp32; q=1,2: many slices; q=3: one slice, column blocks
+    nq = na[q - 1]
+    m = 48
+    nc = list(na)
+    nc[q - 1] = m
+    wa, wc = ka.dense_strides(na, pia), ka.dense_strides(nc, pia)
+    rng = np.random.default_rng(q)
+    a = torch.from_numpy(rng.standard_normal(int(np.prod(na))).astype(dtype)).pin_memory()
+    b = rng.standard_normal(m * nq).astype(dtype)
+    c = torch.full((int(np.prod(nc)),), float("nan"), dtype=a.dtype).pin_memory()
+    if a.numel() * a.element_size() < (64 << 20):
+        pytest.skip("below the pipelining threshold")
+    dt = _lib.F32 if dtype == np.float32 else _lib.F64
+    _lib.ttm_raw(dt, prec, q, 3, a.data_ptr(), na, wa, pia, b.ctypes.data, [m, nq], [1, 2], c.data_ptr(), nc, wc)
+    qh = pia.index(q)
+    inner = int(np.prod([na[pia[r] - 1] for r in range(qh)]))
+    outer = int(np.prod(na)) // (inner * nq)
+    A3 = a.numpy().astype(np.float64).reshape(outer, nq, inner)
+    want = np.matmul(b.astype(np.float64).reshape(nq, m).T, A3).reshape(-1)
+    tol = 1e-5 if prec == _lib.PREC_BF16X3 else (2e-6 if dtype == np.float32 else 1e-13)
+    assert relerr(c.numpy(), want) <= tol

@@ -1,5 +1,6 @@
 // C ABI of the B200 TTM library: argument checks, device planner, staging of
 // host operands, kernel dispatch. Declarations and contract: include/tlibttm.h.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -283,6 +284,162 @@ int classify(const void* ptr, int dev, Where& w)
     return TLIBTTM_OK;
 }
 
+// ---- pipelined staging of large host operands ----------------------------------------------
+// A large TTM with host operands is cut into chunks of whole slices (along `outer`) or, when there
+// are few slices, into column blocks of each slice (along `inner`, 2-D copies). Chunk c is copied
+// in on the copy-in stream, contracted on the compute stream and copied out on the copy-out
+// stream, with a ring of kRing device buffers, so both PCIe directions and the kernels overlap.
+constexpr int kRing = 3;
+constexpr size_t kChunkBytes = size_t(256) << 20;    // target bytes of A per chunk
+constexpr size_t kPipelineMinBytes = size_t(64) << 20;
+
+struct PipeState {
+    std::mutex mu;
+    bool init = false;
+    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    cudaEvent_t ev_in[kRing], ev_comp[kRing], ev_out[kRing], ev_b, ev_user, ev_done;
+    DevBuf a[kRing], c[kRing], b;
+};
+
+std::mutex g_pipe_mu;
+std::unordered_map<int, PipeState*> g_pipes;
+
+PipeState* pipe_for(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_pipe_mu);
+    PipeState*& p = g_pipes[dev];
+    if (!p) p = new PipeState();
+    return p;
+}
+
+cudaError_t pipe_init(PipeState& ps)
+{
+    if (ps.init) return cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&ps.in, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = cudaStreamCreateWithFlags(&ps.comp, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if ((e = cudaStreamCreateWithFlags(&ps.out, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    for (int i = 0; i < kRing; ++i) {
+        if ((e = cudaEventCreateWithFlags(&ps.ev_in[i], cudaEventDisableTiming)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&ps.ev_comp[i], cudaEventDisableTiming)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&ps.ev_out[i], cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    if ((e = cudaEventCreateWithFlags(&ps.ev_b, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&ps.ev_user, cudaEventDisableTiming)) != cudaSuccess) return e;
+    if ((e = cudaEventCreateWithFlags(&ps.ev_done, cudaEventDisableTiming)) != cudaSuccess) return e;
+    ps.init = true;
+    return cudaSuccess;
+}
+
+// True when the pipelined path applies: dense, large, A and C both host memory, and chunkable
+// either along outer (enough slices) or along inner in multiples of 128.
+bool pipeline_applies(const Plan& pl, size_t es, Where wa, Where wc)
+{
+    if (!pl.dense || wa != Where::Host || wc != Where::Host) return false;
+    if (pl.a_elems * es < kPipelineMinBytes) return false;
+    return pl.v.outer >= 8 || pl.v.inner % 128 == 0;
+}
+
+int run_pipelined(const Args& x, Plan& pl, int precision, cudaStream_t user, Where wb, int dev)
+{
+    const size_t es = x.dtype == TLIBTTM_F32 ? sizeof(float) : sizeof(double);
+    const View3 full = pl.v;
+    PipeState& ps = *pipe_for(dev);
+    std::lock_guard<std::mutex> lk(ps.mu);
+    cudaError_t e = pipe_init(ps);
+    if (e != cudaSuccess) return cuda_fail(e, "pipeline set-up");
+
+    // Chunk geometry.
+    const size_t slice_bytes = (size_t)(full.nq * full.inner) * es;
+    const bool by_outer = full.outer >= 8;
+    int64_t kstep = 1, istep = full.inner;
+    if (by_outer) {
+        kstep = std::max<int64_t>(1, (int64_t)(kChunkBytes / slice_bytes));
+        kstep = std::min<int64_t>(kstep, (full.outer + kRing - 1) / kRing);
+    } else {
+        istep = std::max<int64_t>(128, (int64_t)(kChunkBytes / ((size_t)full.nq * es)) / 128 * 128);
+        istep = std::min<int64_t>(istep, full.inner);
+    }
+    const size_t a_chunk = (size_t)(kstep * full.nq * istep) * es;
+    const size_t c_chunk = (size_t)(kstep * full.m * istep) * es;
+    for (int i = 0; i < kRing; ++i) {
+        if (ensure(ps.a[i], a_chunk) != cudaSuccess || ensure(ps.c[i], c_chunk) != cudaSuccess)
+            return fail(TLIBTTM_ERR_ALLOC, "tlibttm: staging allocation failed.");
+    }
+    // Order after the caller's prior work on its stream.
+    if ((e = cudaEventRecord(ps.ev_user, user)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    for (cudaStream_t st : {ps.in, ps.comp, ps.out})
+        if ((e = cudaStreamWaitEvent(st, ps.ev_user, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+
+    const void* bdev = x.b;
+    if (wb == Where::Host) {
+        if (ensure(ps.b, pl.b_elems * es) != cudaSuccess) return fail(TLIBTTM_ERR_ALLOC, "tlibttm: staging allocation for B failed.");
+        if ((e = cudaMemcpyAsync(ps.b.ptr, x.b, pl.b_elems * es, cudaMemcpyHostToDevice, ps.in)) != cudaSuccess)
+            return cuda_fail(e, "copy of B");
+        bdev = ps.b.ptr;
+    }
+    if ((e = cudaEventRecord(ps.ev_b, ps.in)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+    if ((e = cudaStreamWaitEvent(ps.comp, ps.ev_b, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+
+    const char* ha = static_cast<const char*>(x.a);
+    char* hc = static_cast<char*>(x.c);
+    int chunk = 0;
+    int rc = TLIBTTM_OK;
+    for (int64_t k0 = 0; k0 < full.outer && rc == TLIBTTM_OK; k0 += kstep) {
+        const int64_t kn = std::min<int64_t>(kstep, full.outer - k0);
+        for (int64_t i0 = 0; i0 < full.inner && rc == TLIBTTM_OK; i0 += istep, ++chunk) {
+            const int64_t in = std::min<int64_t>(istep, full.inner - i0);
+            const int r = chunk % kRing;
+            if (chunk >= kRing) {
+                // slot r is free once its previous compute and copy-out are done
+                if ((e = cudaStreamWaitEvent(ps.in, ps.ev_comp[r], 0)) != cudaSuccess) return cuda_fail(e, "wait");
+                if ((e = cudaStreamWaitEvent(ps.comp, ps.ev_out[r], 0)) != cudaSuccess) return cuda_fail(e, "wait");
+            }
+            char* da = static_cast<char*>(ps.a[r].ptr);
+            char* dc = static_cast<char*>(ps.c[r].ptr);
+            if (by_outer) {
+                e = cudaMemcpyAsync(da, ha + (size_t)(k0 * full.nq * full.inner) * es, (size_t)(kn * full.nq * full.inner) * es,
+                                    cudaMemcpyHostToDevice, ps.in);
+            } else {
+                e = cudaMemcpy2DAsync(da, (size_t)in * es, ha + (size_t)(k0 * full.nq * full.inner + i0) * es,
+                                      (size_t)full.inner * es, (size_t)in * es, (size_t)full.nq, cudaMemcpyHostToDevice, ps.in);
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "copy of A");
+            if ((e = cudaEventRecord(ps.ev_in[r], ps.in)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+            if ((e = cudaStreamWaitEvent(ps.comp, ps.ev_in[r], 0)) != cudaSuccess) return cuda_fail(e, "wait");
+
+            Args d = x;
+            d.a = da;
+            d.b = bdev;
+            d.c = dc;
+            Plan sub = pl;
+            sub.v.outer = kn;
+            sub.v.inner = in;
+            rc = run_device(d, sub, precision, ps.comp);
+            if (rc) break;
+            if ((e = cudaEventRecord(ps.ev_comp[r], ps.comp)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+            if ((e = cudaStreamWaitEvent(ps.out, ps.ev_comp[r], 0)) != cudaSuccess) return cuda_fail(e, "wait");
+            if (by_outer) {
+                e = cudaMemcpyAsync(hc + (size_t)(k0 * full.m * full.inner) * es, dc, (size_t)(kn * full.m * full.inner) * es,
+                                    cudaMemcpyDeviceToHost, ps.out);
+            } else {
+                e = cudaMemcpy2DAsync(hc + (size_t)(k0 * full.m * full.inner + i0) * es, (size_t)full.inner * es, dc,
+                                      (size_t)in * es, (size_t)in * es, (size_t)full.m, cudaMemcpyDeviceToHost, ps.out);
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "copy of C");
+            if ((e = cudaEventRecord(ps.ev_out[r], ps.out)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        }
+    }
+    for (cudaStream_t st : {ps.in, ps.comp, ps.out}) {
+        cudaError_t e2 = cudaStreamSynchronize(st);
+        if (e2 != cudaSuccess && rc == TLIBTTM_OK) rc = cuda_fail(e2, "cudaStreamSynchronize");
+    }
+    if (rc) return rc;
+    if (tc_read_status())
+        return fail(TLIBTTM_ERR_DEVICE, "tlibttm: a tensor-core kernel gave up on a bounded wait; its output is invalid.");
+    return TLIBTTM_OK;
+}
+
 int run(const Args& x, int precision, void* stream)
 {
     int rc = validate(x);
@@ -302,6 +459,7 @@ int run(const Args& x, int precision, void* stream)
 
     // At least one host operand: stage through the pool and block until done.
     const size_t es = x.dtype == TLIBTTM_F32 ? sizeof(float) : sizeof(double);
+    if (pipeline_applies(pl, es, wa, wc)) return run_pipelined(x, pl, precision, s, wb, dev);
     Pool& pool = pool_for(dev);
     std::lock_guard<std::mutex> lk(pool.mu);
     Args d = x;
