@@ -134,6 +134,63 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p,
                                    float* c, const size_t* nc, const size_t* wc,
                                    void* stream);
 
+/*
+ * Plans: many TTMs prepared once, run many times (an extension; the
+ * reference's closest counterparts are the MKL-only batched_gemm policy,
+ * include/tlib/detail/ttm.h:1321-1403, and ttmpy.ttms,
+ * ttmpy/src/wrapped_ttm.cpp:81-222). A plan records device pointers and
+ * metadata at creation; running it re-reads the current contents of those
+ * buffers. All operands of a plan must be device memory of the current device.
+ */
+typedef struct tlibttm_plan_s tlibttm_plan;
+
+/* One TTM of a batched plan, with the arguments of tlibttm_ttm_f32/_f64. */
+typedef struct tlibttm_problem {
+    unsigned q, p;
+    const void* a; const size_t* na; const size_t* wa; const size_t* pia;
+    const void* b; const size_t* nb; const size_t* pib;
+    void* c; const size_t* nc; const size_t* wc;
+} tlibttm_problem;
+
+/*
+ * Batched plan: `count` independent TTMs of one dtype. Dense problems on the
+ * SIMT paths run in ONE persistent grouped launch whose blocks pull work items
+ * (slice-GEMM tiles or row blocks of small-m problems, largest problems first)
+ * from a device work queue; problems that take the tensor-core path
+ * (precision bf16x3/auto) or that have non-dense strides are launched after it
+ * on the same stream. Errors name the offending problem ("problem 7: ...").
+ */
+int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_problem* problems,
+                         tlibttm_plan** plan);
+
+/*
+ * Chain plan (Tucker projection, ttmpy.ttms): C = A x_{modes[0]} B_0 x_{modes[1]} B_1 ... in
+ * the given order. A has order p, extents na and layout pia (dense); B_s has shape
+ * (ms[s], n) with n the current extent of mode modes[s] and layout pibs[2s..2s+1];
+ * every intermediate and C are dense with layout pia. Intermediates live in
+ * device buffers the plan owns.
+ */
+int tlibttm_plan_chain(int dtype, int precision, unsigned p, const void* a, const size_t* na, const size_t* pia,
+                       unsigned count, const unsigned* modes, const void* const* bs, const size_t* ms,
+                       const size_t* pibs, void* c, tlibttm_plan** plan);
+
+/* Enqueues the plan's launches on `stream`. */
+int tlibttm_plan_run(tlibttm_plan* plan, void* stream);
+
+/*
+ * Runs the plan as a CUDA graph: the first call captures the plan's launches
+ * into a graph and instantiates it, later calls replay it (one launch of the
+ * whole plan). With stream == NULL a stream owned by the plan is used and the
+ * call waits for completion.
+ */
+int tlibttm_plan_run_graph(tlibttm_plan* plan, void* stream);
+
+/* Number of kernel launches one run of the plan performs (grouped + individual). */
+int tlibttm_plan_launches(const tlibttm_plan* plan);
+
+/* Frees the plan, its device buffers and its graph. */
+int tlibttm_plan_destroy(tlibttm_plan* plan);
+
 /* Text of the last error reported on the calling thread ("" if none). */
 const char* tlibttm_last_error(void);
 

@@ -2,6 +2,7 @@
 // host operands, kernel dispatch. Declarations and contract: include/tlibttm.h.
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -33,6 +34,7 @@ const char* kernel_name(int id)
     case K_TC_FP8: return "tc_fp8";
     case K_TC_OZAKI: return "tc_ozaki";
     case K_SPLIT_B: return "split_b";
+    case K_GROUPED: return "grouped";
     default: return "";
     }
 }
@@ -493,6 +495,90 @@ int run(const Args& x, int precision, void* stream)
     return TLIBTTM_OK;
 }
 
+// ---- plans ----------------------------------------------------------------------------------
+struct Single {            // one problem launched on its own inside a plan
+    int dtype;
+    const void* a;
+    const void* b;
+    void* c;
+    Plan pl;
+};
+
+int run_single(Single& sg, int precision, cudaStream_t s)
+{
+    Args x{};
+    x.dtype = sg.dtype;
+    x.a = sg.a;
+    x.b = sg.b;
+    x.c = sg.c;
+    return run_device(x, sg.pl, precision, s);
+}
+
+// Kernels run_device launches for a plan entry (tensor-core paths launch two).
+int launches_of(const Single& sg, int dtype, int precision)
+{
+    if (!sg.pl.dense) return 1;
+    if (sg.pl.v.m <= kSmallM) return 1;
+    int pr = precision == TLIBTTM_PREC_DEFAULT ? g_precision.load() : precision;
+    if (pr == TLIBTTM_PREC_AUTO)
+        pr = (dtype == TLIBTTM_F32 && tc_supported(sg.pl.v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3 : TLIBTTM_PREC_PLAIN;
+    return (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) ? 2 : 1;
+}
+
+}  // namespace
+}  // namespace tlibttm
+
+struct tlibttm_plan_s {
+    int type = 0;          // 0 batched, 1 chain
+    int dtype = 0, precision = 0, dev = 0;
+    // batched
+    std::vector<tlibttm::GroupDesc> descs;
+    tlibttm::GroupDesc* d_desc = nullptr;
+    unsigned long long* d_queue = nullptr;
+    int64_t total = 0;
+    int grid = 0;
+    std::vector<tlibttm::Single> singles;   // individual launches (batched extras, or chain steps)
+    // chain
+    void* bufs[2] = {nullptr, nullptr};
+    // graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t own = nullptr;
+};
+
+namespace tlibttm {
+namespace {
+
+int plan_run_impl(tlibttm_plan* P, cudaStream_t s)
+{
+    int rc;
+    if (P->type == 0 && P->total > 0) {
+        cudaError_t e = cudaMemsetAsync(P->d_queue, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+        if ((rc = note_launch(launch_grouped(P->d_desc, (int)P->descs.size(), P->total, P->d_queue, P->dtype, P->grid, s),
+                              K_GROUPED)))
+            return rc;
+    }
+    for (Single& sg : P->singles)
+        if ((rc = run_single(sg, P->precision, s))) return rc;
+    return TLIBTTM_OK;
+}
+
+void plan_free(tlibttm_plan* P)
+{
+    if (!P) return;
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    if (P->d_desc) cudaFree(P->d_desc);
+    if (P->d_queue) cudaFree(P->d_queue);
+    for (void* b : P->bufs)
+        if (b) cudaFree(b);
+    if (P->own) cudaStreamDestroy(P->own);
+    delete P;
+}
+
+std::string problem_prefix(size_t i) { return "problem " + std::to_string(i) + ": "; }
+
 }  // namespace
 }  // namespace tlibttm
 
@@ -564,6 +650,241 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
     e = launch_tc_noalloc(v, static_cast<cudaStream_t>(stream), &kid);
     if (e == cudaSuccess) ++g_launches;   // split_b_kernel; note_launch counts the main kernel
     return note_launch(e, kid);
+}
+
+int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_problem* problems,
+                         tlibttm_plan** plan)
+{
+    if (!plan) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_batched: plan pointer is null.");
+    *plan = nullptr;
+    if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
+    if (precision < TLIBTTM_PREC_DEFAULT || precision > TLIBTTM_PREC_AUTO)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown precision.");
+    if (count && !problems) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_batched: problems pointer is null.");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    int prec = precision == TLIBTTM_PREC_DEFAULT ? g_precision.load() : precision;
+    std::unique_ptr<tlibttm_plan, void (*)(tlibttm_plan*)> P(new tlibttm_plan_s(), plan_free);
+    P->type = 0;
+    P->dtype = dtype;
+    P->precision = precision;
+    P->dev = dev;
+    const size_t es = dtype == TLIBTTM_F32 ? sizeof(float) : sizeof(double);
+    const int64_t tile = dtype == TLIBTTM_F32 ? kGemmTileF32 : kGemmTileF64;
+    struct Item { GroupDesc d; double cost; };
+    std::vector<Item> items;
+    for (size_t i = 0; i < count; ++i) {
+        const tlibttm_problem& pr = problems[i];
+        Args x{dtype, pr.q, pr.p, pr.a, pr.na, pr.wa, pr.pia, pr.b, pr.nb, pr.pib, pr.c, pr.nc, pr.wc};
+        int rc = validate(x);
+        if (!rc) {
+            Plan pl;
+            rc = make_plan(x, pl);
+            if (!rc) {
+                Where wa, wb, wc;
+                if ((rc = classify(x.a, dev, wa)) || (rc = classify(x.b, dev, wb)) || (rc = classify(x.c, dev, wc))) {
+                } else if (wa != Where::Device || wb != Where::Device || wc != Where::Device) {
+                    rc = fail(TLIBTTM_ERR_ARG, "plans take device operands only.");
+                } else {
+                    View3 v = pl.v;
+                    v.a = x.a;
+                    v.b = x.b;
+                    v.c = x.c;
+                    bool tc = false;
+                    if (pl.dense && v.m > kSmallM && dtype == TLIBTTM_F32) {
+                        if (prec == TLIBTTM_PREC_BF16X3 || prec == TLIBTTM_PREC_AUTO) tc = tc_supported(v, TLIBTTM_PREC_BF16X3);
+                    }
+                    if (!pl.dense || tc) {
+                        P->singles.push_back(Single{dtype, x.a, x.b, x.c, pl});
+                    } else {
+                        GroupDesc d{};
+                        d.a = x.a;
+                        d.b = x.b;
+                        d.c = x.c;
+                        d.outer = v.outer;
+                        d.nq = v.nq;
+                        d.inner = v.inner;
+                        d.m = v.m;
+                        d.b_cm = v.b_cm;
+                        const int64_t M = v.outer * v.inner;
+                        const int64_t rv = 16 / (int64_t)es;
+                        if (v.m <= kSmallM) {
+                            d.kind = 1;
+                            d.tiles_m = ceil_div(M, kGemvRows);
+                            d.tiles_n = 1;
+                        } else {
+                            d.kind = 0;
+                            d.tiles_m = ceil_div(M, tile);
+                            d.tiles_n = ceil_div(v.m, tile);
+                            const bool ak = v.inner == 1;
+                            bool vec = (reinterpret_cast<uintptr_t>(v.a) % 16 == 0) && (reinterpret_cast<uintptr_t>(v.c) % 16 == 0);
+                            vec = vec && (ak ? (v.nq % rv == 0 && v.m % rv == 0) : (v.inner % rv == 0));
+                            d.flags = (ak ? 1 : 0) | (vec ? 2 : 0);
+                        }
+                        items.push_back(Item{d, (double)(d.tiles_m * d.tiles_n) * (double)v.nq});
+                    }
+                }
+            }
+        }
+        if (rc) return fail(rc, problem_prefix(i) + g_err);
+    }
+    std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+    int64_t first = 0;
+    for (Item& it : items) {
+        it.d.first = first;
+        first += it.d.tiles_m * it.d.tiles_n;
+        P->descs.push_back(it.d);
+    }
+    P->total = first;
+    if (!P->descs.empty()) {
+        if ((e = cudaMalloc(&P->d_desc, P->descs.size() * sizeof(GroupDesc))) != cudaSuccess ||
+            (e = cudaMalloc(&P->d_queue, sizeof(unsigned long long))) != cudaSuccess)
+            return fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_batched: device allocation failed.");
+        if ((e = cudaMemcpy(P->d_desc, P->descs.data(), P->descs.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return cuda_fail(e, "plan upload");
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t grid = (int64_t)sms * grouped_blocks_per_sm(dtype);
+        P->grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, P->total));
+    }
+    if (!P->singles.empty() && (e = tc_prepare_device()) != cudaSuccess) return cuda_fail(e, "tensor-core state");
+    *plan = P.release();
+    return TLIBTTM_OK;
+}
+
+int tlibttm_plan_chain(int dtype, int precision, unsigned p, const void* a, const size_t* na, const size_t* pia,
+                       unsigned count, const unsigned* modes, const void* const* bs, const size_t* ms,
+                       const size_t* pibs, void* c, tlibttm_plan** plan)
+{
+    if (!plan) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_chain: plan pointer is null.");
+    *plan = nullptr;
+    if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
+    if (precision < TLIBTTM_PREC_DEFAULT || precision > TLIBTTM_PREC_AUTO)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown precision.");
+    if (count == 0) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_chain: the chain is empty.");
+    if (!na || !pia || !modes || !bs || !ms || !pibs)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_chain: a metadata pointer is null.");
+    if (p == 0) return fail(TLIBTTM_ERR_ARG, "Error in tlib::tensor_times_matrix: input tensor order should be greater zero.");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    std::unique_ptr<tlibttm_plan, void (*)(tlibttm_plan*)> P(new tlibttm_plan_s(), plan_free);
+    P->type = 1;
+    P->dtype = dtype;
+    P->precision = precision;
+    P->dev = dev;
+    const size_t es = dtype == TLIBTTM_F32 ? sizeof(float) : sizeof(double);
+    std::vector<size_t> cur(na, na + p), layout(pia, pia + p);
+    // sizes of the intermediates (steps 0..count-2)
+    size_t max_mid = 0;
+    {
+        std::vector<size_t> n = cur;
+        for (unsigned s = 0; s + 1 < count; ++s) {
+            if (modes[s] == 0 || modes[s] > p) break;
+            n[modes[s] - 1] = ms[s];
+            size_t tot = 1;
+            for (size_t x : n) tot *= x;
+            max_mid = std::max(max_mid, tot);
+        }
+    }
+    if (count > 1) {
+        for (int i = 0; i < 2; ++i)
+            if ((e = cudaMalloc(&P->bufs[i], std::max<size_t>(max_mid, 1) * es)) != cudaSuccess)
+                return fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_chain: device allocation failed.");
+    }
+    const void* in = a;
+    for (unsigned s = 0; s < count; ++s) {
+        std::vector<size_t> nc = cur;
+        const unsigned q = modes[s];
+        if (q >= 1 && q <= p) nc[q - 1] = ms[s];
+        std::vector<size_t> wa(p), wc(p), nb(2);
+        tlib::ttm::detail::compute_strides(cur.begin(), cur.end(), layout.begin(), wa.begin());
+        tlib::ttm::detail::compute_strides(nc.begin(), nc.end(), layout.begin(), wc.begin());
+        nb[0] = ms[s];
+        nb[1] = (q >= 1 && q <= p) ? cur[q - 1] : 0;
+        void* out = (s + 1 == count) ? c : P->bufs[s & 1];
+        // B_s's own column count is checked against the current extent through nb[1]: the caller
+        // states B_s's rows only, so its columns are the current extent by construction.
+        Args x{dtype, q, p, in, cur.data(), wa.data(), layout.data(), bs[s], nb.data(), pibs + 2 * s, out, nc.data(),
+               wc.data()};
+        int rc = validate(x);
+        if (!rc) {
+            Plan pl;
+            rc = make_plan(x, pl);
+            if (!rc) {
+                Where w1, w2, w3;
+                if ((rc = classify(in, dev, w1)) || (rc = classify(bs[s], dev, w2)) || (rc = classify(out, dev, w3))) {
+                } else if (w1 != Where::Device || w2 != Where::Device || w3 != Where::Device) {
+                    rc = fail(TLIBTTM_ERR_ARG, "plans take device operands only.");
+                } else {
+                    P->singles.push_back(Single{dtype, in, bs[s], out, pl});
+                }
+            }
+        }
+        if (rc) return fail(rc, "step " + std::to_string(s) + ": " + g_err);
+        in = out;
+        cur = nc;
+    }
+    if ((e = tc_prepare_device()) != cudaSuccess) return cuda_fail(e, "tensor-core state");
+    *plan = P.release();
+    return TLIBTTM_OK;
+}
+
+int tlibttm_plan_run(tlibttm_plan* plan, void* stream)
+{
+    if (!plan) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_run: plan is null.");
+    return plan_run_impl(plan, static_cast<cudaStream_t>(stream));
+}
+
+int tlibttm_plan_run_graph(tlibttm_plan* plan, void* stream)
+{
+    if (!plan) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_run_graph: plan is null.");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if (!s) {
+        if (!plan->own && (e = cudaStreamCreateWithFlags(&plan->own, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(e, "cudaStreamCreate");
+        s = plan->own;
+    }
+    if (!plan->exec) {
+        if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return cuda_fail(e, "cudaStreamBeginCapture");
+        const unsigned long long before = g_launches;
+        int rc = plan_run_impl(plan, s);
+        g_launches = before;   // capture enqueues nothing; the replay below is what runs
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(s, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        plan->graph = g;
+        if ((e = cudaGraphInstantiate(&plan->exec, g, 0)) != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    if ((e = cudaGraphLaunch(plan->exec, s)) != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+    g_launches += (unsigned long long)tlibttm_plan_launches(plan);
+    if (!stream) {
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+        if (tc_read_status())
+            return fail(TLIBTTM_ERR_DEVICE, "tlibttm: a tensor-core kernel gave up on a bounded wait; its output is invalid.");
+    }
+    return TLIBTTM_OK;
+}
+
+int tlibttm_plan_launches(const tlibttm_plan* plan)
+{
+    if (!plan) return 0;
+    int n = (plan->type == 0 && plan->total > 0) ? 1 : 0;
+    for (const Single& sg : plan->singles) n += launches_of(sg, plan->dtype, plan->precision);
+    return n;
+}
+
+int tlibttm_plan_destroy(tlibttm_plan* plan)
+{
+    plan_free(plan);
+    return TLIBTTM_OK;
 }
 
 const char* tlibttm_last_error(void) { return g_err.c_str(); }

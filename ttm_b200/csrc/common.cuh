@@ -44,6 +44,21 @@ struct StridedProblem {
     int64_t wc[kMaxOrder];    // C strides (mode order)
 };
 
+// One problem of a grouped launch (device copy built by the host plan).
+struct GroupDesc {
+    const void* a;
+    const void* b;
+    void* c;
+    int64_t outer, nq, inner, m;
+    int b_cm;
+    int kind;          // 0: slice-GEMM tiles, 1: rows of the small-m kernel
+    int flags;         // slice-GEMM: bit 0 A K-major (inner == 1), bit 1 16-byte vector access
+    int pad;
+    int64_t tiles_m;   // slice-GEMM: row tiles; small-m: blocks of 256 rows
+    int64_t tiles_n;   // slice-GEMM: column tiles; small-m: 1
+    int64_t first;     // index of the problem's first work item
+};
+
 // Kernel identifiers (for diagnostics and launch counting).
 enum KernelId : int {
     K_NONE = 0,
@@ -55,6 +70,7 @@ enum KernelId : int {
     K_TC_FP8,
     K_TC_OZAKI,
     K_SPLIT_B,
+    K_GROUPED,
     K_COUNT
 };
 
@@ -65,6 +81,15 @@ cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_rowdot(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_strided(const StridedProblem& sp, int dtype, cudaStream_t s);
+
+// Grouped launch: `count` problems, `total` work items pulled from the device counter `queue`
+// (which must be zero at launch) by a persistent grid of `grid` blocks.
+cudaError_t launch_grouped(const GroupDesc* d_desc, int count, int64_t total, unsigned long long* queue, int dtype,
+                           int grid, cudaStream_t s);
+// Row / column tile sizes of the slice-GEMM for an element type, and rows per small-m work item.
+constexpr int kGemmTileF32 = 128, kGemmTileF64 = 64, kGemvRows = 256;
+// Blocks per SM the grouped kernel is launched with.
+int grouped_blocks_per_sm(int dtype);
 
 // Largest m handled by the small-m bandwidth kernels.
 constexpr int64_t kSmallM = 16;

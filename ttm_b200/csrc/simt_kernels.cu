@@ -64,8 +64,16 @@ __device__ __forceinline__ double fma_t(double a, double b, double c) { return _
 //          by the host).
 //   BCM  : B column-major.
 // ---------------------------------------------------------------------------------------------
+template <typename T>
+struct GemmSmem {
+    static constexpr int RV = 16 / sizeof(T);
+    __align__(16) T As[2][8][32 * RV];
+    __align__(16) T Bs[2][8][32 * RV];
+};
+
+// One BM x BN output tile (rows m0.., columns n0..) of the slice-GEMM, all 256 threads of the block.
 template <typename T, bool AK, bool VEC, bool BCM>
-__global__ void __launch_bounds__(256) simt_gemm_kernel(View3 v)
+__device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0, GemmSmem<T>& sm)
 {
     constexpr int RV = 16 / sizeof(T);   // elements per 16-byte vector
     constexpr int BM = 32 * RV, BN = 32 * RV, BK = 8;
@@ -79,16 +87,14 @@ __global__ void __launch_bounds__(256) simt_gemm_kernel(View3 v)
     // B tile: BK x BN, scalar loads.
     constexpr int LB = BN * BK / NT;
 
-    __shared__ __align__(16) T As[2][BK][BM];
-    __shared__ __align__(16) T Bs[2][BK][BN];
+    auto& As = sm.As;
+    auto& Bs = sm.Bs;
 
     const T* __restrict__ A = static_cast<const T*>(v.a);
     const T* __restrict__ B = static_cast<const T*>(v.b);
     T* __restrict__ Cp = static_cast<T*>(v.c);
     const int64_t inner = v.inner, nq = v.nq, m = v.m;
     const int64_t M = v.outer * inner;
-    const int64_t m0 = (int64_t)blockIdx.x * BM;
-    const int64_t n0 = (int64_t)blockIdx.y * BN;
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
 
@@ -255,6 +261,14 @@ __global__ void __launch_bounds__(256) simt_gemm_kernel(View3 v)
     }
 }
 
+template <typename T, bool AK, bool VEC, bool BCM>
+__global__ void __launch_bounds__(256) simt_gemm_kernel(View3 v)
+{
+    constexpr int RV = 16 / sizeof(T);
+    __shared__ GemmSmem<T> sm;
+    gemm_tile<T, AK, VEC, BCM>(v, (int64_t)blockIdx.x * (32 * RV), (int64_t)blockIdx.y * (32 * RV), sm);
+}
+
 // ---------------------------------------------------------------------------------------------
 // colvec: small m, W consecutive i per thread (W | inner).
 // ---------------------------------------------------------------------------------------------
@@ -403,6 +417,101 @@ __global__ void __launch_bounds__(256) strided_kernel(StridedProblem sp)
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// grouped: many independent TTMs in one persistent launch. Blocks pull work items from a device
+// counter; an item is one slice-GEMM tile of a problem (m > 16) or a block of 256 rows of a
+// small-m problem. Problems are ordered largest first by the host, so the tail is short.
+// ---------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void gemv_rows(const View3& v, int64_t row0, T* bsm)
+{
+    constexpr int MB = 16;
+    constexpr int LB = (int)(sizeof(GemmSmem<T>) / sizeof(T)) / MB;
+    const T* __restrict__ A = static_cast<const T*>(v.a);
+    const T* __restrict__ B = static_cast<const T*>(v.b);
+    T* __restrict__ Cp = static_cast<T*>(v.c);
+    const int64_t inner = v.inner, nq = v.nq, m = v.m;
+    const int64_t M = v.outer * inner;
+    const int64_t row = row0 + threadIdx.x;
+    const bool valid = row < M;
+    const int64_t k = valid ? row / inner : 0;
+    const int64_t i = valid ? row - k * inner : 0;
+    const T* ap = A + k * inner * nq + i;
+    T acc[MB];
+#pragma unroll
+    for (int j = 0; j < MB; ++j) acc[j] = T(0);
+    for (int64_t l0 = 0; l0 < nq; l0 += LB) {
+        const int lc = (int)((nq - l0) < LB ? (nq - l0) : LB);
+        __syncthreads();
+        for (int e = threadIdx.x; e < lc * MB; e += blockDim.x) {
+            const int l = e / MB, j = e % MB;
+            const int64_t gl = l0 + l;
+            bsm[e] = (j < m) ? (v.b_cm ? B[j + gl * m] : B[j * nq + gl]) : T(0);
+        }
+        __syncthreads();
+        if (valid) {
+            for (int l = 0; l < lc; ++l) {
+                const T a = __ldg(ap + (l0 + l) * inner);
+#pragma unroll
+                for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bsm[l * MB + j], acc[j]);
+            }
+        }
+    }
+    if (valid) {
+        T* cp = Cp + k * inner * m + i;
+#pragma unroll
+        for (int j = 0; j < MB; ++j)
+            if (j < m) cp[j * inner] = acc[j];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) grouped_kernel(const GroupDesc* __restrict__ desc, int count, int64_t total,
+                                                      unsigned long long* queue)
+{
+    constexpr int RV = 16 / sizeof(T);
+    constexpr int BM = 32 * RV, BN = 32 * RV;
+    __shared__ GemmSmem<T> sm;
+    __shared__ int64_t item_s;
+    for (;;) {
+        if (threadIdx.x == 0) item_s = (int64_t)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const int64_t item = item_s;
+        if (item >= total) break;
+        int lo = 0, hi = count - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (desc[mid].first <= item) lo = mid;
+            else hi = mid - 1;
+        }
+        const GroupDesc g = desc[lo];
+        const int64_t local = item - g.first;
+        View3 v;
+        v.a = g.a;
+        v.b = g.b;
+        v.c = g.c;
+        v.outer = g.outer;
+        v.nq = g.nq;
+        v.inner = g.inner;
+        v.m = g.m;
+        v.b_cm = g.b_cm;
+        if (g.kind == 0) {
+            const int64_t m0 = (local % g.tiles_m) * BM, n0 = (local / g.tiles_m) * BN;
+            const bool ak = g.flags & 1, vec = g.flags & 2;
+            if (ak) {
+                if (vec) { if (g.b_cm) gemm_tile<T, true, true, true>(v, m0, n0, sm); else gemm_tile<T, true, true, false>(v, m0, n0, sm); }
+                else     { if (g.b_cm) gemm_tile<T, true, false, true>(v, m0, n0, sm); else gemm_tile<T, true, false, false>(v, m0, n0, sm); }
+            } else {
+                if (vec) { if (g.b_cm) gemm_tile<T, false, true, true>(v, m0, n0, sm); else gemm_tile<T, false, true, false>(v, m0, n0, sm); }
+                else     { if (g.b_cm) gemm_tile<T, false, false, true>(v, m0, n0, sm); else gemm_tile<T, false, false, false>(v, m0, n0, sm); }
+            }
+        } else {
+            gemv_rows<T>(v, local * kGemvRows, reinterpret_cast<T*>(&sm));
+        }
+        __syncthreads();
+    }
+}
+
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 template <typename T>
@@ -494,6 +603,22 @@ cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s)
 cudaError_t launch_rowdot(const View3& v, int dtype, cudaStream_t s)
 {
     return dtype == 0 ? rowdot_dispatch<float>(v, s) : rowdot_dispatch<double>(v, s);
+}
+
+int grouped_blocks_per_sm(int dtype)
+{
+    int n = 0;
+    cudaError_t e = dtype == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_kernel<float>, 256, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_kernel<double>, 256, 0);
+    return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+cudaError_t launch_grouped(const GroupDesc* d_desc, int count, int64_t total, unsigned long long* queue, int dtype,
+                           int grid, cudaStream_t s)
+{
+    if (dtype == 0) grouped_kernel<float><<<grid, 256, 0, s>>>(d_desc, count, total, queue);
+    else grouped_kernel<double><<<grid, 256, 0, s>>>(d_desc, count, total, queue);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_strided(const StridedProblem& sp, int dtype, cudaStream_t s)

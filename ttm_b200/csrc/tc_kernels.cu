@@ -878,6 +878,15 @@ cudaError_t launch_tc_noalloc(const View3& v, cudaStream_t s, int* kid)
     return run_bf16x3(v, sy.image, sy.status, sms, s);
 }
 
+cudaError_t tc_prepare_device()
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    DevState* st = nullptr;
+    return state_for(dev, st);
+}
+
 int tc_read_status()
 {
     int dev = 0;

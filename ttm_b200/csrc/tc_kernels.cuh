@@ -12,6 +12,10 @@ bool tc_supported(const View3& v, int precision);
 // identifier of the main kernel launched.
 cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid);
 
+// Creates the per-device state of the tensor-core paths ahead of time (so that a later stream
+// capture does not need to allocate it).
+cudaError_t tc_prepare_device();
+
 // Frees device state owned by the tensor-core paths on the current device.
 void tc_release_buffers();
 
