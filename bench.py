@@ -43,6 +43,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched and Tucker workloads")
     return ap.parse_args()
 
 
@@ -198,6 +199,65 @@ class ClockSampler:
                 if any(r[3].replace('.', '', 1).isdigit() for r in rows) else None}
 
 
+def _time_graph(plan, stream, reps=5):
+    import torch
+    for _ in range(2):
+        plan.run_graph(stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        plan.run_graph(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def run_extra_workloads(dev, stream):
+    """Batched: 512 independent fp32 TTMs drawn as in the batched workload (seed 0), one plan,
+    replayed as a CUDA graph. Tucker: A (192,192,192,192) fp32 x U_k^T (32,192) on modes 1..4 in
+    sequence, one chain plan, replayed as a CUDA graph. Precision auto (FP32-accurate)."""
+    import math
+    import torch
+    from ttm_b200 import workloads
+    from ttm_b200.plans import BatchPlan, ChainPlan
+    out = {}
+    probs = workloads.problems(512, seed=0)
+    entries = []
+    gen = torch.Generator(device=dev).manual_seed(1)
+    for pr in probs:
+        na, q, m = pr["na"], pr["q"], pr["m"]
+        n_a = math.prod(na)
+        A = torch.randn(n_a, device=dev, generator=gen)
+        B = torch.randn(m, na[q - 1], device=dev, generator=gen)
+        Cc = torch.empty(n_a // na[q - 1] * m, device=dev)
+        entries.append(dict(q=q, A=A, B=B, C=Cc, na=na, pia=pr["pia"], m=m))
+    plan = BatchPlan(entries, precision="auto")
+    t = _time_graph(plan, stream)
+    fl = sum(workloads.flops(p) for p in probs)
+    by = sum(workloads.io_bytes(p) for p in probs)
+    out["batched_512"] = {"tflops": fl / t / 1e12, "gbs": by / t / 1e9, "ms": 1e3 * t, "problems": 512,
+                          "launches_per_run": plan.launches, "flop": fl, "bytes": by,
+                          "note": "one batched plan (grouped persistent launch + tensor-core launches), CUDA graph replay"}
+    plan.close()
+    del entries
+    S, r = 192, 32
+    A = torch.randn(S ** 4, device=dev, generator=gen)
+    Us = [torch.randn(r, S, device=dev, generator=gen) for _ in range(4)]
+    Cc = torch.empty(r ** 4, device=dev)
+    chain = ChainPlan(A, [S] * 4, [1, 2, 3, 4], [1, 2, 3, 4], Us, Cc, precision="auto")
+    t = _time_graph(chain, stream)
+    fl = sum(2.0 * r * (r ** k) * (S ** (4 - k)) for k in range(4))
+    by = 4.0 * sum((r ** k) * (S ** (4 - k)) + (r ** (k + 1)) * (S ** (3 - k)) + r * S for k in range(4))
+    out["tucker_192"] = {"tflops": fl / t / 1e12, "gbs": by / t / 1e9, "ms": 1e3 * t, "flop": fl, "bytes": by,
+                         "launches_per_run": chain.launches,
+                         "note": "A 192^4 x U_k^T (32,192), k = 1..4, one chain plan, CUDA graph replay"}
+    chain.close()
+    del A, Us, Cc
+    torch.cuda.empty_cache()
+    return out
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -317,6 +377,10 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         plain_tflops = flops_per_step(S) / (e0.elapsed_time(e1) / 1e3) / 1e12
 
+    extra = {}
+    if not args.no_extra:
+        extra = run_extra_workloads(dev, stream)
+
     # end to end through the C ABI with pinned host buffers: copies inside the timed region
     e2e = None
     if not args.no_e2e:
@@ -373,6 +437,7 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,
+            "extra": extra,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -41,3 +41,14 @@ def test_ttms_sequences():
     assert [r for r, _ in _ttms_sequence(2, 4, Bs, "backward")] == [4, 3, 1]
     # 1/n - 1/m: mode1 1/3-1/6=.167, mode3 1/2-1/7=.357, mode4 1/4-1/9=.139
     assert [r for r, _ in _ttms_sequence(2, 4, Bs, "optimal")] == [4, 1, 3]
+
+
+def test_ttms_mode_q_plus_1_mismatch_is_runtime_error():
+    """The reference does not compare the matrix of mode q+1 in its own checks; the mismatch
+    surfaces from tlib::ttm as RuntimeError (needs no GPU: rejected before any launch)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("the chain runs on the GPU")
+    A = np.zeros((3, 2, 4, 5))
+    with pytest.raises(RuntimeError, match="contraction dimension of A and B are not equal"):
+        tp.ttms(1, A, [np.zeros((6, 3)), np.zeros((7, 4)), np.zeros((9, 5))])

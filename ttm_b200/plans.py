@@ -131,6 +131,16 @@ class ChainPlan(_Plan):
         L = _lib.lib()
         _declare(L)
         n = len(modes)
+        if len(Bs) != n:
+            raise ValueError("ChainPlan: one matrix per mode is required.")
+        ext = list(na)
+        for r, b in zip(modes, Bs):
+            if not 1 <= r <= len(na) or b.dim() != 2 or int(b.shape[1]) != ext[r - 1]:
+                raise ValueError(f"ChainPlan: matrix for mode {r} must have {ext[r - 1] if 1 <= r <= len(na) else '?'} "
+                                 "columns (the current extent of that mode).")
+            ext[r - 1] = int(b.shape[0])
+        if C_out.numel() != int(__import__("math").prod(ext)) or A.numel() != int(__import__("math").prod(na)):
+            raise ValueError("ChainPlan: A or C does not have the element count its extents imply.")
         mods = (C.c_uint * n)(*modes)
         bptr = (C.c_void_p * n)(*[b.data_ptr() for b in Bs])
         ms = _lib.sz([b.shape[0] for b in Bs])

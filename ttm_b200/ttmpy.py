@@ -210,28 +210,49 @@ def ttms(q, A, Bs, order="forward", precision="default"):
 
     ``order`` is "forward" (ascending modes), "backward" (descending) or
     "optimal" (ascending 1/n_k - 1/m_k, i.e. the most shrinking factors first).
-    Numpy inputs are moved to the GPU once; all intermediates stay in device
-    memory and only the final tensor returns to the host.
+    The whole chain runs as one plan (include/tlibttm.h, tlibttm_plan_chain):
+    numpy inputs are moved to the GPU once, intermediates stay in device
+    buffers the plan owns, and only the final tensor returns to the host.
     """
     q = int(q)
     p = _ttms_check(q, A, Bs, order)
     seq = _ttms_sequence(q, p, Bs, order)
-    if _is_torch(A):
+    if torch is None or not torch.cuda.is_available():
         c = A
         for r, k in seq:
             c = ttm(r, c, Bs[k], precision)
         return c
-    if torch is None or not torch.cuda.is_available():
-        c = np.asarray(A)
-        for r, k in seq:
-            c = ttm(r, c, Bs[k], precision)
-        return c
-    A = np.asarray(A)
-    if A.dtype not in (np.float32, np.float64):
-        A = A.astype(np.float64)
-    dev = torch.device("cuda", torch.cuda.current_device())
-    c = torch.from_numpy(np.ascontiguousarray(A)).to(dev)
+    from .plans import ChainPlan
+    host = not _is_torch(A)
+    if host:
+        A = np.asarray(A)
+        if A.dtype not in (np.float32, np.float64):
+            A = A.astype(np.float64)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        tA = torch.from_numpy(np.ascontiguousarray(A)).to(dev)
+    else:
+        tA = A.contiguous()
+        if tA.dtype not in (torch.float32, torch.float64):
+            tA = tA.to(torch.float64)
+        dev = tA.device
+    dt = tA.dtype
+    # C-ordered tensor: mode r has extent shape[r-1]; layout is last-order (p, ..., 1).
+    na = list(tA.shape)
+    pia = list(range(p, 0, -1))
+    bs = []
+    ext = list(na)
     for r, k in seq:
-        b = torch.from_numpy(np.ascontiguousarray(np.asarray(Bs[k], dtype=A.dtype))).to(dev)
-        c = ttm(r, c, b, precision)
-    return c.cpu().numpy()
+        b = Bs[k]
+        if int(b.shape[1]) != ext[r - 1]:
+            # what tlib::ttm raises for this contraction (include/tlib/ttm.h:80)
+            raise RuntimeError("Error in tlib::tensor_times_matrix: contraction dimension of A and B are not equal.")
+        b = b.to(device=dev, dtype=dt) if _is_torch(b) else torch.from_numpy(np.asarray(b)).to(device=dev, dtype=dt)
+        bs.append(b.contiguous())
+        ext[r - 1] = int(b.shape[0])
+    out = torch.empty(ext, device=dev, dtype=dt)
+    with torch.cuda.device(dev):
+        plan = ChainPlan(tA.reshape(-1), na, pia, [r for r, _ in seq], bs, out.reshape(-1), precision=precision)
+        plan.run()
+        torch.cuda.current_stream(dev).synchronize()
+        plan.close()
+    return out.cpu().numpy() if host else out
