@@ -496,6 +496,10 @@ int run(const Args& x, int precision, void* stream)
 }
 
 // ---- plans ----------------------------------------------------------------------------------
+// Under precision auto, a batched problem takes the tensor-core path only from this many
+// elements of A on; smaller ones run inside the grouped launch.
+constexpr int64_t kAutoTcMinElems = int64_t(1) << 22;
+
 struct Single {            // one problem launched on its own inside a plan
     int dtype;
     const void* a;
@@ -693,7 +697,11 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                     v.c = x.c;
                     bool tc = false;
                     if (pl.dense && v.m > kSmallM && dtype == TLIBTTM_F32) {
-                        if (prec == TLIBTTM_PREC_BF16X3 || prec == TLIBTTM_PREC_AUTO) tc = tc_supported(v, TLIBTTM_PREC_BF16X3);
+                        // bf16x3 is asked for explicitly: every supported problem takes it. Under auto,
+                        // only large problems do; small ones are cheaper inside the grouped launch.
+                        if (prec == TLIBTTM_PREC_BF16X3) tc = tc_supported(v, TLIBTTM_PREC_BF16X3);
+                        if (prec == TLIBTTM_PREC_AUTO)
+                            tc = tc_supported(v, TLIBTTM_PREC_BF16X3) && v.outer * v.inner * v.nq >= kAutoTcMinElems;
                     }
                     if (!pl.dense || tc) {
                         P->singles.push_back(Single{dtype, x.a, x.b, x.c, pl});
@@ -711,7 +719,19 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                         const int64_t rv = 16 / (int64_t)es;
                         if (v.m <= kSmallM) {
                             d.kind = 1;
-                            d.tiles_m = ceil_div(M, kGemvRows);
+                            const bool al = (reinterpret_cast<uintptr_t>(v.a) % 16 == 0) && (reinterpret_cast<uintptr_t>(v.c) % 16 == 0);
+                            // work items: 256 rows (contiguous fibres) or 32*W rows (strided fibres,
+                            // W = 16-byte width when aligned) -- the tile sizes of rowdot / colvec
+                            if (v.inner == 1) {
+                                d.flags = 1 | ((reinterpret_cast<uintptr_t>(v.a) % 16 == 0 && v.nq % rv == 0) ? 2 : 0);
+                                d.tiles_m = ceil_div(M, kGemvRows);
+                            } else if (al && v.inner % rv == 0) {
+                                d.flags = 2;
+                                d.tiles_m = ceil_div(M, 8 * 32 * rv);
+                            } else {
+                                d.flags = 0;
+                                d.tiles_m = ceil_div(M, 8 * 32);
+                            }
                             d.tiles_n = 1;
                         } else {
                             d.kind = 0;
@@ -722,7 +742,10 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                             vec = vec && (ak ? (v.nq % rv == 0 && v.m % rv == 0) : (v.inner % rv == 0));
                             d.flags = (ak ? 1 : 0) | (vec ? 2 : 0);
                         }
-                        items.push_back(Item{d, (double)(d.tiles_m * d.tiles_n) * (double)v.nq});
+                        // cost ~ work-item count x work per item, for a largest-first order
+                        const double per_item = d.kind == 0 ? (double)v.nq * tile * tile
+                                                            : (double)v.nq * (d.flags & 1 ? kGemvRows : 8 * 32 * (d.flags & 2 ? rv : 1)) * 16;
+                        items.push_back(Item{d, (double)(d.tiles_m * d.tiles_n) * per_item});
                     }
                 }
             }

@@ -52,9 +52,10 @@ struct GroupDesc {
     int64_t outer, nq, inner, m;
     int b_cm;
     int kind;          // 0: slice-GEMM tiles, 1: rows of the small-m kernel
-    int flags;         // slice-GEMM: bit 0 A K-major (inner == 1), bit 1 16-byte vector access
+    int flags;         // bit 0: fibres contiguous (inner == 1); bit 1: 16-byte vector access
     int pad;
-    int64_t tiles_m;   // slice-GEMM: row tiles; small-m: blocks of 256 rows
+    int64_t tiles_m;   // slice-GEMM: row tiles; small-m: blocks of 256 rows (256 * 16/sizeof(T) when
+                       // strided fibres are read with 16-byte loads)
     int64_t tiles_n;   // slice-GEMM: column tiles; small-m: 1
     int64_t first;     // index of the problem's first work item
 };

@@ -270,21 +270,36 @@ __global__ void __launch_bounds__(256) simt_gemm_kernel(View3 v)
 }
 
 // ---------------------------------------------------------------------------------------------
-// colvec: small m, W consecutive i per thread (W | inner).
+// colvec: small m (<= MB), strided fibres (inner >= 2). Each lane owns W consecutive rows (i of
+// one slice; 16-byte loads when W = 16/sizeof(T)). The block's 8 warps are split into 8/LS row
+// chunks of LS warps each; the LS warps of a chunk split the l loop (warp w takes l = w, w+LS,
+// ...) and reduce through shared memory at the end. LS = 1 gives 8*32*W rows per block and no
+// reduction (problems with many rows); LS = 8 gives 32*W rows per block and 8 independent load
+// streams per row chunk (problems with few rows). B is staged in shared memory as [l][MB].
 // ---------------------------------------------------------------------------------------------
-template <typename T, int MB, int W>
-__global__ void __launch_bounds__(256) colvec_kernel(View3 v)
-{
-    constexpr int LBS = 8192 / MB;   // l values per shared-memory chunk (32 KB f32 / 64 KB f64 max)
-    constexpr int LB = (LBS * MB * sizeof(T) > 32768) ? 32768 / (MB * sizeof(T)) : LBS;
-    __shared__ __align__(16) T Bs[LB][MB];
+constexpr int kColWarps = 8;
 
+template <typename T, int MB>
+struct ColvecSmem {
+    static constexpr int MBP = MB < 4 ? 4 : MB;
+    static constexpr int LB = (32768 / (MBP * (int)sizeof(T))) < 512 ? 32768 / (MBP * (int)sizeof(T)) : 512;  // l per staged chunk of B
+    __align__(16) T bs[LB][MBP];
+    __align__(16) T red[kColWarps][32 * (16 / sizeof(T))];
+};
+
+template <typename T, int MB, int W, int LS>
+__device__ __forceinline__ void colvec_tile(const View3& v, int64_t row0, ColvecSmem<T, MB>& sm)
+{
+    constexpr int LB = ColvecSmem<T, MB>::LB;
+    constexpr int MBP = MB < 4 ? 4 : MB;
     const T* __restrict__ A = static_cast<const T*>(v.a);
     const T* __restrict__ B = static_cast<const T*>(v.b);
     T* __restrict__ Cp = static_cast<T*>(v.c);
     const int64_t inner = v.inner, nq = v.nq, m = v.m;
     const int64_t M = v.outer * inner;
-    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * W;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int chunk = warp / LS, part = warp % LS;
+    const int64_t row = row0 + ((int64_t)chunk * 32 + lane) * W;
     const bool valid = row < M;
     const int64_t k = valid ? row / inner : 0;
     const int64_t i = valid ? row - k * inner : 0;
@@ -299,91 +314,169 @@ __global__ void __launch_bounds__(256) colvec_kernel(View3 v)
     for (int64_t l0 = 0; l0 < nq; l0 += LB) {
         const int lc = (int)((nq - l0) < LB ? (nq - l0) : LB);
         __syncthreads();
-        for (int e = threadIdx.x; e < lc * MB; e += blockDim.x) {
-            const int l = e / MB, j = e % MB;
+        for (int e = threadIdx.x; e < lc * MBP; e += blockDim.x) {
+            const int l = e / MBP, j = e % MBP;
             const int64_t gl = l0 + l;
-            Bs[l][j] = (j < m) ? (v.b_cm ? B[j + gl * m] : B[j * nq + gl]) : T(0);
+            sm.bs[l][j] = (j < m) ? (v.b_cm ? B[j + gl * m] : B[j * nq + gl]) : T(0);
         }
         __syncthreads();
         if (valid) {
-            const T* p = ap + l0 * inner;
 #pragma unroll 4
-            for (int l = 0; l < lc; ++l) {
+            for (int l = part; l < lc; l += LS) {
                 T a[W];
-                load_vec<T, W>(a, p + (int64_t)l * inner);
+                load_vec<T, W>(a, ap + (l0 + l) * inner);
+                T bj[MBP];
+                if constexpr (MBP * sizeof(T) % 16 == 0) {
 #pragma unroll
-                for (int j = 0; j < MB; ++j) {
-                    const T bj = Bs[l][j];
+                    for (int c = 0; c < MBP * (int)sizeof(T) / 16; ++c) {
+                        typename V16<T>::type t = *reinterpret_cast<const typename V16<T>::type*>(&sm.bs[l][c * (16 / sizeof(T))]);
 #pragma unroll
-                    for (int w = 0; w < W; ++w) acc[j][w] = fma_t(a[w], bj, acc[j][w]);
+                        for (int e = 0; e < (int)(16 / sizeof(T)); ++e) bj[c * (16 / sizeof(T)) + e] = reinterpret_cast<const T*>(&t)[e];
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < MBP; ++j) bj[j] = sm.bs[l][j];
                 }
+#pragma unroll
+                for (int j = 0; j < MB; ++j)
+#pragma unroll
+                    for (int w = 0; w < W; ++w) acc[j][w] = fma_t(a[w], bj[j], acc[j][w]);
             }
         }
     }
-    if (valid) {
-        T* cp = Cp + k * inner * m + i;
+    T* cp = Cp + k * inner * m + i;
+    if constexpr (LS == 1) {
+        if (valid) {
 #pragma unroll
-        for (int j = 0; j < MB; ++j)
-            if (j < m) store_vec<T, W>(cp + j * inner, acc[j]);
+            for (int j = 0; j < MB; ++j)
+                if (j < m) store_vec<T, W>(cp + j * inner, acc[j]);
+        }
+    } else {
+        // Reduce the LS warps' partial sums, one output column at a time.
+#pragma unroll
+        for (int j = 0; j < MB; ++j) {
+            if (j >= m) break;
+            __syncthreads();
+#pragma unroll
+            for (int w = 0; w < W; ++w) sm.red[warp][lane * W + w] = acc[j][w];
+            __syncthreads();
+            if (part == 0 && valid) {
+                T r[W];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    T t = T(0);
+#pragma unroll
+                    for (int q = 0; q < LS; ++q) t += sm.red[chunk * LS + q][lane * W + w];
+                    r[w] = t;
+                }
+                store_vec<T, W>(cp + j * inner, r);
+            }
+        }
     }
 }
 
-// ---------------------------------------------------------------------------------------------
-// rowdot: small m, inner == 1. A group of G lanes reads one contiguous fibre A[k][0..nq).
-// ---------------------------------------------------------------------------------------------
-template <typename T, int MB, int G, int W, bool BSMEM>
-__global__ void __launch_bounds__(256) rowdot_kernel(View3 v)
+template <typename T, int MB, int W, int LS>
+__global__ void __launch_bounds__(256) colvec_kernel(View3 v)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Bs = reinterpret_cast<T*>(smem_raw);   // [m][nq], row-major in j
+    __shared__ ColvecSmem<T, MB> sm;
+    colvec_tile<T, MB, W, LS>(v, (int64_t)blockIdx.x * (kColWarps / LS) * 32 * W, sm);
+}
 
+// ---------------------------------------------------------------------------------------------
+// rowdot: small m (<= MB), contiguous fibres (inner == 1): C[k][j] = sum_l A[k][l] B(j,l).
+// Each warp owns 32 rows; the block walks l in chunks of LC = 128/sizeof(T): every warp copies
+// its 32 x LC tile of A into padded shared memory with coalesced 16-byte loads, the block stages
+// B[l][MB] for the chunk, then each lane accumulates its own row from shared memory.
+// ---------------------------------------------------------------------------------------------
+template <typename T, int MB>
+struct RowdotSmem {
+    static constexpr int LC = 128 / sizeof(T);          // l per chunk (one 128-byte line per row)
+    T a[8][32][LC + 1];                                  // per warp, padded rows
+    __align__(16) T bs[LC][MB < 4 ? 4 : MB];
+};
+
+template <typename T, int MB, bool VEC>
+__device__ __forceinline__ void rowdot_tile(const View3& v, int64_t row0, RowdotSmem<T, MB>& sm)
+{
+    constexpr int LC = RowdotSmem<T, MB>::LC;
+    constexpr int MBP = MB < 4 ? 4 : MB;
+    constexpr int RV = 16 / sizeof(T);
     const T* __restrict__ A = static_cast<const T*>(v.a);
     const T* __restrict__ B = static_cast<const T*>(v.b);
     T* __restrict__ Cp = static_cast<T*>(v.c);
     const int64_t nq = v.nq, m = v.m, rows = v.outer;
-
-    if (BSMEM) {
-        for (int64_t e = threadIdx.x; e < m * nq; e += blockDim.x) {
-            const int64_t j = e / nq, l = e - j * nq;
-            Bs[e] = v.b_cm ? B[j + l * m] : B[j * nq + l];
-        }
-        __syncthreads();
-    }
-    const int lane = threadIdx.x % G;
-    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
-    const bool valid = row < rows;
-
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t wrow0 = row0 + warp * 32;
+    const int64_t row = wrow0 + lane;
     T acc[MB];
 #pragma unroll
     for (int j = 0; j < MB; ++j) acc[j] = T(0);
-    if (valid) {
-        const T* ap = A + row * nq;
-        for (int64_t l = (int64_t)lane * W; l < nq; l += (int64_t)G * W) {
-            T a[W];
-            load_vec<T, W>(a, ap + l);
+
+    for (int64_t l0 = 0; l0 < nq; l0 += LC) {
+        const int lc = (int)((nq - l0) < LC ? (nq - l0) : LC);
+        __syncthreads();
+        // B chunk
+        for (int e = threadIdx.x; e < LC * MBP; e += blockDim.x) {
+            const int l = e / MBP, j = e % MBP;
+            const int64_t gl = l0 + l;
+            sm.bs[l][j] = (j < m && l < lc) ? (v.b_cm ? B[j + gl * m] : B[j * nq + gl]) : T(0);
+        }
+        // this warp's A tile: rows wrow0 .. +31, columns l0 .. l0+LC-1
+        if (VEC) {
+            // (LC / RV) lanes per row, 32 / (LC / RV) rows per step
+            constexpr int LPR = LC / RV, RPS = 32 / LPR;
+            const int r_in = lane / LPR, c = (lane % LPR) * RV;
 #pragma unroll
-            for (int j = 0; j < MB; ++j) {
-                if (j < m) {
+            for (int r = r_in; r < 32; r += RPS) {
+                const int64_t gr = wrow0 + r;
+                T x[RV];
+                if (gr < rows && c < lc) load_vec<T, RV>(x, A + gr * nq + l0 + c);
+                else {
 #pragma unroll
-                    for (int w = 0; w < W; ++w) {
-                        const T bj = BSMEM ? Bs[j * nq + l + w]
-                                           : __ldg(v.b_cm ? B + j + (l + w) * m : B + j * nq + l + w);
-                        acc[j] = fma_t(a[w], bj, acc[j]);
-                    }
+                    for (int e = 0; e < RV; ++e) x[e] = T(0);
                 }
+#pragma unroll
+                for (int e = 0; e < RV; ++e) sm.a[warp][r][c + e] = x[e];
+            }
+        } else {
+            for (int r = 0; r < 32; ++r) {
+                const int64_t gr = wrow0 + r;
+                for (int c = lane; c < LC; c += 32)
+                    sm.a[warp][r][c] = (gr < rows && c < lc) ? __ldg(A + gr * nq + l0 + c) : T(0);
             }
         }
+        __syncthreads();
+#pragma unroll 8
+        for (int l = 0; l < lc; ++l) {
+            const T a = sm.a[warp][lane][l];
+            T bj[MBP];
+            if constexpr (MBP * sizeof(T) % 16 == 0) {
+#pragma unroll
+                for (int cc = 0; cc < MBP * (int)sizeof(T) / 16; ++cc) {
+                    typename V16<T>::type t = *reinterpret_cast<const typename V16<T>::type*>(&sm.bs[l][cc * RV]);
+#pragma unroll
+                    for (int e = 0; e < RV; ++e) bj[cc * RV + e] = reinterpret_cast<const T*>(&t)[e];
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < MBP; ++j) bj[j] = sm.bs[l][j];
+            }
+#pragma unroll
+            for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bj[j], acc[j]);
+        }
     }
-    // All lanes (valid or not) take part in the shuffles: G divides 32.
-#pragma unroll
-    for (int off = G / 2; off > 0; off >>= 1)
-#pragma unroll
-        for (int j = 0; j < MB; ++j) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], off);
-    if (valid && lane == 0) {
+    if (row < rows) {
 #pragma unroll
         for (int j = 0; j < MB; ++j)
             if (j < m) Cp[row * m + j] = acc[j];
     }
+}
+
+template <typename T, int MB, bool VEC>
+__global__ void __launch_bounds__(256) rowdot_kernel(View3 v)
+{
+    __shared__ RowdotSmem<T, MB> sm;
+    rowdot_tile<T, MB, VEC>(v, (int64_t)blockIdx.x * 256, sm);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -423,45 +516,24 @@ __global__ void __launch_bounds__(256) strided_kernel(StridedProblem sp)
 // small-m problem. Problems are ordered largest first by the host, so the tail is short.
 // ---------------------------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ void gemv_rows(const View3& v, int64_t row0, T* bsm)
+union GroupedSmem {
+    GemmSmem<T> gemm;
+    ColvecSmem<T, 16> col;
+    RowdotSmem<T, 16> row;
+};
+
+template <typename T, int MB>
+__device__ __forceinline__ void grouped_small(const View3& v, int flags, int64_t local, GroupedSmem<T>& sm)
 {
-    constexpr int MB = 16;
-    constexpr int LB = (int)(sizeof(GemmSmem<T>) / sizeof(T)) / MB;
-    const T* __restrict__ A = static_cast<const T*>(v.a);
-    const T* __restrict__ B = static_cast<const T*>(v.b);
-    T* __restrict__ Cp = static_cast<T*>(v.c);
-    const int64_t inner = v.inner, nq = v.nq, m = v.m;
-    const int64_t M = v.outer * inner;
-    const int64_t row = row0 + threadIdx.x;
-    const bool valid = row < M;
-    const int64_t k = valid ? row / inner : 0;
-    const int64_t i = valid ? row - k * inner : 0;
-    const T* ap = A + k * inner * nq + i;
-    T acc[MB];
-#pragma unroll
-    for (int j = 0; j < MB; ++j) acc[j] = T(0);
-    for (int64_t l0 = 0; l0 < nq; l0 += LB) {
-        const int lc = (int)((nq - l0) < LB ? (nq - l0) : LB);
-        __syncthreads();
-        for (int e = threadIdx.x; e < lc * MB; e += blockDim.x) {
-            const int l = e / MB, j = e % MB;
-            const int64_t gl = l0 + l;
-            bsm[e] = (j < m) ? (v.b_cm ? B[j + gl * m] : B[j * nq + gl]) : T(0);
-        }
-        __syncthreads();
-        if (valid) {
-            for (int l = 0; l < lc; ++l) {
-                const T a = __ldg(ap + (l0 + l) * inner);
-#pragma unroll
-                for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bsm[l * MB + j], acc[j]);
-            }
-        }
-    }
-    if (valid) {
-        T* cp = Cp + k * inner * m + i;
-#pragma unroll
-        for (int j = 0; j < MB; ++j)
-            if (j < m) cp[j * inner] = acc[j];
+    constexpr int RV = 16 / sizeof(T);
+    auto& col = reinterpret_cast<ColvecSmem<T, MB>&>(sm.col);
+    auto& row = reinterpret_cast<RowdotSmem<T, MB>&>(sm.row);
+    if (flags & 1) {
+        if (flags & 2) rowdot_tile<T, MB, true>(v, local * 256, row);
+        else rowdot_tile<T, MB, false>(v, local * 256, row);
+    } else {
+        if (flags & 2) colvec_tile<T, MB, RV, 1>(v, local * kColWarps * 32 * RV, col);
+        else colvec_tile<T, MB, 1, 1>(v, local * kColWarps * 32, col);
     }
 }
 
@@ -471,7 +543,7 @@ __global__ void __launch_bounds__(256) grouped_kernel(const GroupDesc* __restric
 {
     constexpr int RV = 16 / sizeof(T);
     constexpr int BM = 32 * RV, BN = 32 * RV;
-    __shared__ GemmSmem<T> sm;
+    __shared__ GroupedSmem<T> sm;
     __shared__ int64_t item_s;
     for (;;) {
         if (threadIdx.x == 0) item_s = (int64_t)atomicAdd(queue, 1ull);
@@ -499,14 +571,18 @@ __global__ void __launch_bounds__(256) grouped_kernel(const GroupDesc* __restric
             const int64_t m0 = (local % g.tiles_m) * BM, n0 = (local / g.tiles_m) * BN;
             const bool ak = g.flags & 1, vec = g.flags & 2;
             if (ak) {
-                if (vec) { if (g.b_cm) gemm_tile<T, true, true, true>(v, m0, n0, sm); else gemm_tile<T, true, true, false>(v, m0, n0, sm); }
-                else     { if (g.b_cm) gemm_tile<T, true, false, true>(v, m0, n0, sm); else gemm_tile<T, true, false, false>(v, m0, n0, sm); }
+                if (vec) { if (g.b_cm) gemm_tile<T, true, true, true>(v, m0, n0, sm.gemm); else gemm_tile<T, true, true, false>(v, m0, n0, sm.gemm); }
+                else     { if (g.b_cm) gemm_tile<T, true, false, true>(v, m0, n0, sm.gemm); else gemm_tile<T, true, false, false>(v, m0, n0, sm.gemm); }
             } else {
-                if (vec) { if (g.b_cm) gemm_tile<T, false, true, true>(v, m0, n0, sm); else gemm_tile<T, false, true, false>(v, m0, n0, sm); }
-                else     { if (g.b_cm) gemm_tile<T, false, false, true>(v, m0, n0, sm); else gemm_tile<T, false, false, false>(v, m0, n0, sm); }
+                if (vec) { if (g.b_cm) gemm_tile<T, false, true, true>(v, m0, n0, sm.gemm); else gemm_tile<T, false, true, false>(v, m0, n0, sm.gemm); }
+                else     { if (g.b_cm) gemm_tile<T, false, false, true>(v, m0, n0, sm.gemm); else gemm_tile<T, false, false, false>(v, m0, n0, sm.gemm); }
             }
         } else {
-            gemv_rows<T>(v, local * kGemvRows, reinterpret_cast<T*>(&sm));
+            if (g.m <= 1) grouped_small<T, 1>(v, g.flags, local, sm);
+            else if (g.m <= 2) grouped_small<T, 2>(v, g.flags, local, sm);
+            else if (g.m <= 4) grouped_small<T, 4>(v, g.flags, local, sm);
+            else if (g.m <= 8) grouped_small<T, 8>(v, g.flags, local, sm);
+            else grouped_small<T, 16>(v, g.flags, local, sm);
         }
         __syncthreads();
     }
@@ -538,18 +614,25 @@ cudaError_t simt_gemm_dispatch(const View3& v, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <typename T, int W, int LS>
+cudaError_t colvec_dispatch_ls(const View3& v, cudaStream_t s)
+{
+    const int64_t M = v.outer * v.inner;
+    dim3 grid((unsigned)ceil_div(M, (kColWarps / LS) * 32 * W)), block(256);
+    if (v.m <= 1) colvec_kernel<T, 1, W, LS><<<grid, block, 0, s>>>(v);
+    else if (v.m <= 2) colvec_kernel<T, 2, W, LS><<<grid, block, 0, s>>>(v);
+    else if (v.m <= 4) colvec_kernel<T, 4, W, LS><<<grid, block, 0, s>>>(v);
+    else if (v.m <= 8) colvec_kernel<T, 8, W, LS><<<grid, block, 0, s>>>(v);
+    else colvec_kernel<T, 16, W, LS><<<grid, block, 0, s>>>(v);
+    return cudaGetLastError();
+}
+
+// Few rows (fewer than ~32 warps of rows per SM): split the l loop across warps.
 template <typename T, int W>
 cudaError_t colvec_dispatch_w(const View3& v, cudaStream_t s)
 {
-    const int64_t M = v.outer * v.inner;
-    const int64_t threads = ceil_div(M, W);
-    dim3 grid((unsigned)ceil_div(threads, 256)), block(256);
-    if (v.m <= 1) colvec_kernel<T, 1, W><<<grid, block, 0, s>>>(v);
-    else if (v.m <= 2) colvec_kernel<T, 2, W><<<grid, block, 0, s>>>(v);
-    else if (v.m <= 4) colvec_kernel<T, 4, W><<<grid, block, 0, s>>>(v);
-    else if (v.m <= 8) colvec_kernel<T, 8, W><<<grid, block, 0, s>>>(v);
-    else colvec_kernel<T, 16, W><<<grid, block, 0, s>>>(v);
-    return cudaGetLastError();
+    const int64_t row_warps = ceil_div(v.outer * v.inner, 32 * W);
+    return row_warps < 148 * 32 ? colvec_dispatch_ls<T, W, 8>(v, s) : colvec_dispatch_ls<T, W, 1>(v, s);
 }
 
 template <typename T>
@@ -560,32 +643,24 @@ cudaError_t colvec_dispatch(const View3& v, cudaStream_t s)
     return vec ? colvec_dispatch_w<T, RV>(v, s) : colvec_dispatch_w<T, 1>(v, s);
 }
 
-template <typename T, int MB, int G, int W>
-cudaError_t rowdot_launch(const View3& v, cudaStream_t s)
+template <typename T, bool VEC>
+cudaError_t rowdot_dispatch_v(const View3& v, cudaStream_t s)
 {
-    const size_t bbytes = (size_t)(v.m * v.nq) * sizeof(T);
-    const bool bsm = bbytes <= 48 * 1024;
-    const int64_t threads = v.outer * G;
-    dim3 grid((unsigned)ceil_div(threads, 256)), block(256);
-    if (bsm) rowdot_kernel<T, MB, G, W, true><<<grid, block, bbytes, s>>>(v);
-    else rowdot_kernel<T, MB, G, W, false><<<grid, block, 0, s>>>(v);
+    dim3 grid((unsigned)ceil_div(v.outer, 256)), block(256);
+    if (v.m <= 1) rowdot_kernel<T, 1, VEC><<<grid, block, 0, s>>>(v);
+    else if (v.m <= 2) rowdot_kernel<T, 2, VEC><<<grid, block, 0, s>>>(v);
+    else if (v.m <= 4) rowdot_kernel<T, 4, VEC><<<grid, block, 0, s>>>(v);
+    else if (v.m <= 8) rowdot_kernel<T, 8, VEC><<<grid, block, 0, s>>>(v);
+    else rowdot_kernel<T, 16, VEC><<<grid, block, 0, s>>>(v);
     return cudaGetLastError();
-}
-
-template <typename T, int MB>
-cudaError_t rowdot_dispatch_m(const View3& v, cudaStream_t s)
-{
-    constexpr int RV = 16 / sizeof(T);
-    const bool vec = aligned16(v.a) && (v.nq % RV == 0);
-    const bool wide = v.nq >= 32 * RV;
-    if (vec) return wide ? rowdot_launch<T, MB, 32, RV>(v, s) : rowdot_launch<T, MB, 4, RV>(v, s);
-    return wide ? rowdot_launch<T, MB, 32, 1>(v, s) : rowdot_launch<T, MB, 4, 1>(v, s);
 }
 
 template <typename T>
 cudaError_t rowdot_dispatch(const View3& v, cudaStream_t s)
 {
-    return v.m <= 4 ? rowdot_dispatch_m<T, 4>(v, s) : rowdot_dispatch_m<T, 16>(v, s);
+    constexpr int RV = 16 / sizeof(T);
+    const bool vec = aligned16(v.a) && (v.nq % RV == 0);
+    return vec ? rowdot_dispatch_v<T, true>(v, s) : rowdot_dispatch_v<T, false>(v, s);
 }
 
 }  // namespace
