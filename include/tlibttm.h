@@ -135,6 +135,52 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p,
                                    void* stream);
 
 /*
+ * Schedules: the kernel choices the planner makes, exposed so that a tuner can
+ * time them (an extension; the reference's counterpart is its choice of
+ * policy tags, include/tlib/detail/ttm.h:1408-1474, the `combined` heuristic).
+ * All but TC_BF16X3 compute in the I/O type with exact FMA.
+ */
+enum tlibttm_schedule {
+    TLIBTTM_SCHED_HEURISTIC = 0,   /* the planner's built-in choice (as tlibttm_ttm_ex, PLAIN) */
+    TLIBTTM_SCHED_SIMT_GEMM = 1,   /* slice-GEMM on FFMA/DFMA, any m */
+    TLIBTTM_SCHED_COLS = 2,        /* small-m kernel for strided fibres, rows spread over warps (m <= 16, inner >= 2) */
+    TLIBTTM_SCHED_COLS_SPLIT = 3,  /* small-m kernel for strided fibres, l split over 8 warps (m <= 16, inner >= 2) */
+    TLIBTTM_SCHED_ROWS = 4,        /* small-m kernel for contiguous fibres (m <= 16, q == pia[0]) */
+    TLIBTTM_SCHED_TC_BF16X3 = 5,   /* tensor-core bf16x3, float only (FP32-accurate, not exact; m > 16) */
+    TLIBTTM_SCHED_COUNT = 6
+};
+
+/* Runs one TTM with a given schedule (all operands device memory, A and C dense). */
+int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p,
+                      const void* a, const size_t* na, const size_t* wa, const size_t* pia,
+                      const void* b, const size_t* nb, const size_t* pib,
+                      void* c, const size_t* nc, const size_t* wc,
+                      void* stream);
+
+/* 1 if `schedule` can run a dense TTM with these extents, layout, mode and m; else 0. */
+int tlibttm_schedule_valid(int dtype, int schedule, unsigned q, unsigned p, const size_t* na, const size_t* pia,
+                           size_t m);
+
+/*
+ * Kernels of the learned schedule selector (no counterpart in the reference):
+ * a multilayer perceptron over float32 device buffers, activations
+ * [batch][features] row-major, weights [out][in].
+ *   forward   y = act(x w^T + bias), act = ReLU when relu != 0
+ *   backward  dz = dy * act'(y) (into the caller's dz buffer), dw = dz^T x,
+ *             db = column sums of dz, dx = dz w (skipped when dx is NULL)
+ *   mse_grad  dy = 2 (y - t) mask / count (inv_count = 1/count), loss += mean masked error^2
+ *   adam      one Adam step (bias-corrected with `step`, counted from 1)
+ */
+int tlibttm_mlp_forward(const float* x, const float* w, const float* bias, float* y, int batch, int in, int out,
+                        int relu, void* stream);
+int tlibttm_mlp_backward(const float* x, const float* w, const float* y, const float* dy, float* dz, float* dx,
+                         float* dw, float* db, int batch, int in, int out, int relu, void* stream);
+int tlibttm_mlp_mse_grad(const float* y, const float* t, const float* mask, float* dy, float* loss, int n,
+                         float inv_count, void* stream);
+int tlibttm_mlp_adam(float* p, const float* g, float* m, float* v, int n, float lr, float beta1, float beta2, float eps,
+                     int step, void* stream);
+
+/*
  * Plans: many TTMs prepared once, run many times (an extension; the
  * reference's closest counterparts are the MKL-only batched_gemm policy,
  * include/tlib/detail/ttm.h:1321-1403, and ttmpy.ttms,

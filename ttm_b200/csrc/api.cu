@@ -617,6 +617,80 @@ int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p, const void*
     return run(x, precision, stream);
 }
 
+static bool sched_valid_view(int dtype, int schedule, const View3& v)
+{
+    switch (schedule) {
+    case TLIBTTM_SCHED_HEURISTIC:
+    case TLIBTTM_SCHED_SIMT_GEMM: return true;
+    case TLIBTTM_SCHED_COLS:
+    case TLIBTTM_SCHED_COLS_SPLIT: return v.m <= kSmallM && v.inner >= 2;
+    case TLIBTTM_SCHED_ROWS: return v.m <= kSmallM && v.inner == 1;
+    case TLIBTTM_SCHED_TC_BF16X3: return dtype == TLIBTTM_F32 && tc_supported(v, TLIBTTM_PREC_BF16X3);
+    default: return false;
+    }
+}
+
+int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p, const void* a, const size_t* na,
+                      const size_t* wa, const size_t* pia, const void* b, const size_t* nb, const size_t* pib,
+                      void* c, const size_t* nc, const size_t* wc, void* stream)
+{
+    if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
+    if (schedule < 0 || schedule >= TLIBTTM_SCHED_COUNT) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown schedule.");
+    Args x{dtype, q, p, a, na, wa, pia, b, nb, pib, c, nc, wc};
+    int rc = validate(x);
+    if (rc) return rc;
+    Plan pl;
+    if ((rc = make_plan(x, pl))) return rc;
+    if (!pl.dense) return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm_ttm_sched: A and C must be dense under their layout.");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    Where w1, w2, w3;
+    if ((rc = classify(a, dev, w1)) || (rc = classify(b, dev, w2)) || (rc = classify(c, dev, w3))) return rc;
+    if (w1 != Where::Device || w2 != Where::Device || w3 != Where::Device)
+        return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_sched: a, b and c must be device memory.");
+    View3 v = pl.v;
+    v.a = a;
+    v.b = b;
+    v.c = c;
+    if (!sched_valid_view(dtype, schedule, v))
+        return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm_ttm_sched: the schedule cannot run this problem.");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    switch (schedule) {
+    case TLIBTTM_SCHED_HEURISTIC: return run_device(x, pl, TLIBTTM_PREC_PLAIN, s);
+    case TLIBTTM_SCHED_SIMT_GEMM: return note_launch(launch_simt_gemm(v, dtype, s), K_SIMT_GEMM);
+    case TLIBTTM_SCHED_COLS: return note_launch(launch_colvec_ls(v, dtype, 1, s), K_COLVEC);
+    case TLIBTTM_SCHED_COLS_SPLIT: return note_launch(launch_colvec_ls(v, dtype, 8, s), K_COLVEC);
+    case TLIBTTM_SCHED_ROWS: return note_launch(launch_rowdot(v, dtype, s), K_ROWDOT);
+    default: {
+        int kid = K_NONE;
+        e = launch_tc(v, TLIBTTM_PREC_BF16X3, s, &kid);
+        if (e == cudaSuccess) ++g_launches;
+        return note_launch(e, kid);
+    }
+    }
+}
+
+int tlibttm_schedule_valid(int dtype, int schedule, unsigned q, unsigned p, const size_t* na, const size_t* pia,
+                           size_t m)
+{
+    if (!na || !pia || p == 0 || q == 0 || q > p) return 0;
+    if (!tlib::ttm::detail::is_valid_shape(na, na + p) || !tlib::ttm::detail::is_valid_layout(pia, pia + p) || m == 0)
+        return 0;
+    unsigned qh = 0;
+    while (pia[qh] != q) ++qh;
+    View3 v{};
+    v.inner = 1;
+    v.outer = 1;
+    for (unsigned r = 0; r < qh; ++r) v.inner *= (int64_t)na[pia[r] - 1];
+    for (unsigned r = qh + 1; r < p; ++r) v.outer *= (int64_t)na[pia[r] - 1];
+    v.nq = (int64_t)na[q - 1];
+    v.m = (int64_t)m;
+    alignas(16) static const float aligned_probe[4] = {0, 0, 0, 0};
+    v.a = aligned_probe;   // alignment of the real operands is checked again when the schedule runs
+    return sched_valid_view(dtype, schedule, v) ? 1 : 0;
+}
+
 // No counterpart in the reference: the bf16x3 contraction without any device
 // allocation (declaration and contract in include/tlibttm.h).
 int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const size_t* na, const size_t* wa,

@@ -80,6 +80,8 @@ const char* kernel_name(int id);
 // Launchers (simt_kernels.cu). Return cudaSuccess or the launch error.
 cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s);
+// colvec with an explicit l split over warps (1 or 8).
+cudaError_t launch_colvec_ls(const View3& v, int dtype, int ls, cudaStream_t s);
 cudaError_t launch_rowdot(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_strided(const StridedProblem& sp, int dtype, cudaStream_t s);
 

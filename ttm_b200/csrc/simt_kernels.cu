@@ -675,6 +675,19 @@ cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s)
     return dtype == 0 ? colvec_dispatch<float>(v, s) : colvec_dispatch<double>(v, s);
 }
 
+cudaError_t launch_colvec_ls(const View3& v, int dtype, int ls, cudaStream_t s)
+{
+    constexpr int RF = 4, RD = 2;
+    if (dtype == 0) {
+        const bool vec = aligned16(v.a) && aligned16(v.c) && (v.inner % RF == 0);
+        if (vec) return ls == 8 ? colvec_dispatch_ls<float, RF, 8>(v, s) : colvec_dispatch_ls<float, RF, 1>(v, s);
+        return ls == 8 ? colvec_dispatch_ls<float, 1, 8>(v, s) : colvec_dispatch_ls<float, 1, 1>(v, s);
+    }
+    const bool vec = aligned16(v.a) && aligned16(v.c) && (v.inner % RD == 0);
+    if (vec) return ls == 8 ? colvec_dispatch_ls<double, RD, 8>(v, s) : colvec_dispatch_ls<double, RD, 1>(v, s);
+    return ls == 8 ? colvec_dispatch_ls<double, 1, 8>(v, s) : colvec_dispatch_ls<double, 1, 1>(v, s);
+}
+
 cudaError_t launch_rowdot(const View3& v, int dtype, cudaStream_t s)
 {
     return dtype == 0 ? rowdot_dispatch<float>(v, s) : rowdot_dispatch<double>(v, s);

@@ -73,6 +73,8 @@ def _check_q_p(q, p, fn):
 
 
 def _ttm_numpy(q, A, B, precision):
+    if precision == "tuned":
+        precision = "plain"
     A = np.asarray(A)
     p = A.ndim
     _check_q_p(q, p, "ttm")
@@ -138,6 +140,19 @@ def _ttm_torch(q, A, B, precision):
     wc = _dense_strides(nc, pia)
     C = torch.empty_strided(nc, wc, dtype=A.dtype, device=A.device)
     stream = torch.cuda.current_stream(A.device).cuda_stream if A.is_cuda else 0
+    if precision == "tuned" and A.is_cuda and _dense_strides(na, pia) == wa:
+        # the learned schedule selector picks among the exact kernels (float32 may also take bf16x3)
+        from . import selector
+        pr = dict(p=p, na=na, q=q, pia=pia, m=nb[0])
+        allowed = {1, 2, 3, 4, 5} if A.dtype == torch.float32 else {1, 2, 3, 4}
+        with torch.cuda.device(A.device):
+            sched, _ = selector.default_selector(A.device).choose(pr, allowed, _dtype_id(A.dtype))
+            _lib.check(selector.lib().tlibttm_ttm_sched(_dtype_id(A.dtype), sched, q, p, A.data_ptr(), _lib.sz(na),
+                                                        _lib.sz(wa), _lib.sz(pia), B.data_ptr(), _lib.sz(nb),
+                                                        _lib.sz(pib), C.data_ptr(), _lib.sz(nc), _lib.sz(wc), stream))
+        return C
+    if precision == "tuned":
+        precision = "auto" if A.dtype == torch.float32 else "plain"
     if A.is_cuda:
         with torch.cuda.device(A.device):
             _lib.ttm_raw(_dtype_id(A.dtype), _prec(precision), q, p, A.data_ptr(), na, wa, pia,
@@ -153,8 +168,9 @@ def ttm(q, A, B, precision="default"):
 
     C(i1..j..ip) = sum_{iq} A(i1..iq..ip) * B(j, iq); q is one-based.
     ``precision`` selects the arithmetic ("default", "plain", "bf16x3",
-    "fp8", "ozaki", "auto"); "default" is the library-wide setting (plain
-    unless changed).
+    "auto", or "tuned"); "default" is the library-wide setting (plain unless
+    changed). "tuned" lets the learned schedule selector pick the kernel for
+    device tensors (FP32-accurate for float32, exact for float64).
     """
     q = int(q)
     if _is_torch(A):
