@@ -272,6 +272,7 @@ def run_ours(args):
     import torch.distributed as dist
 
     from ttm_b200 import _lib
+    from ttm_b200.replicas import barrier as replica_barrier, max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -300,9 +301,7 @@ def run_ours(args):
                      out.data_ptr(), na, wa, sh)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
+        replica_barrier(dev)
 
     # correctness spot check of this exact configuration (sampled fibres vs float64) before timing
     relerr = {}
@@ -349,11 +348,7 @@ def run_ours(args):
         t1.record(stream)
         barrier()
     launches = _lib.launch_count() - launches0
-    elapsed = t0.elapsed_time(t1) / 1e3
-    if world > 1:
-        tt = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
+    elapsed = max_over_ranks(t0.elapsed_time(t1) / 1e3, dev)
     per_launch = [s.elapsed_time(e) / 1e3 for s, e in ev]
     clocks = clk.summary()
 
@@ -400,11 +395,7 @@ def run_ours(args):
         for _ in range(args.e2e_steps):
             e2e_step()
         barrier()
-        te = time.perf_counter() - t0
-        if world > 1:
-            tt = torch.tensor([te], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = max_over_ranks(time.perf_counter() - t0, dev)
         e2e = {"value": world * flops_per_step(S) * args.e2e_steps / te / 1e12, "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(4 * (4 * n + 4 * S * S)), "d2h_bytes_per_step": int(4 * 4 * n),
                "steps": args.e2e_steps}
