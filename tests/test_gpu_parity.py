@@ -118,11 +118,60 @@ def test_layout_mode_sweep_vs_oracle(cuda, oracle_c, dtype):
     assert worst <= (1e-13 if dtype == np.float64 else 2e-6), worst
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_stream_cols_box_shapes(cuda, oracle_c, dtype):
+    """The TMA-fed small-m kernel packs KB = P / IB slices into one box when inner is small, folds
+    a large inner into (i mod IB, i / IB) boxes when there are few slices, and splits the l range
+    (partial tiles added by the last unit) when tiles are few or B is large. Cover each box mode,
+    partial boxes in i, k and l, B restaged per unit, every m bucket and both B layouts; shapes
+    the kernel declines (mostly out-of-range fill) must take another kernel."""
+    import torch
+    from ttm_b200.selector import lib
+    rng = np.random.default_rng(21)
+    shapes = [(4, 300, 5, 1), (4, 1000, 70, 16), (8, 257, 33, 8), (12, 700, 16, 3), (36, 120, 9, 2),
+              (64, 37, 33, 8), (64, 130, 1000, 1), (100, 256, 16, 4), (128, 37, 33, 8), (260, 256, 5, 1),
+              (256, 4, 3000, 16), (512, 2, 1000, 1), (4096, 1, 37, 8), (1536, 2, 9, 2), (65536, 1, 3, 1),
+              (8192, 3, 20, 4), (96, 1, 50, 16), (4, 3, 16, 3)]
+    if dtype == np.float64:
+        shapes += [(2, 512, 7, 2), (6, 256, 9, 8)]
+    dt = _lib.F32 if dtype == np.float32 else _lib.F64
+    taken = []
+    for n, (inner, outer, nq, m) in enumerate(shapes):
+        na = [inner, nq, outer]
+        nc = [inner, m, outer]
+        pia = [1, 2, 3]
+        md = dict(na=na, wa=ka.dense_strides(na, pia), pia=pia, nb=[m, nq], pib=[1, 2] if n % 2 else [2, 1],
+                  nc=nc, wc=ka.dense_strides(nc, pia))
+        a = rng.standard_normal(int(np.prod(na))).astype(dtype)
+        b = rng.standard_normal(m * nq).astype(dtype)
+        ta, tb = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+        tc = torch.full((int(np.prod(nc)),), float("nan"), dtype=ta.dtype, device=cuda)
+        rc = lib().tlibttm_ttm_sched(dt, 6, 2, 3, ta.data_ptr(), _lib.sz(na), _lib.sz(md["wa"]), _lib.sz(pia),
+                                     tb.data_ptr(), _lib.sz(md["nb"]), _lib.sz(md["pib"]), tc.data_ptr(), _lib.sz(nc),
+                                     _lib.sz(md["wc"]), None)
+        valid = lib().tlibttm_schedule_valid(dt, 6, 2, 3, _lib.sz(na), _lib.sz(pia), m)
+        assert rc == (0 if valid else _lib.ERR_UNSUPPORTED), (inner, outer, nq, m, rc)
+        if not valid:
+            continue
+        assert _lib.last_kernel() == "stream_cols"
+        taken.append((inner, outer))
+        c = tc.cpu().numpy()
+        ref = np.zeros(int(np.prod(nc)), dtype=dtype)
+        oracle_c.ttm(2, a, na, md["wa"], pia, b, md["nb"], md["pib"], ref, nc, md["wc"])
+        assert relerr(c, ref) <= (1e-14 if dtype == np.float64 else 2e-6), (inner, outer, nq, m)
+    # the folded boxes, the restaged B and the narrow-row boxes were all exercised
+    for want in ((4096, 1), (65536, 1), (512, 2), (256, 4), (4, 1000)):
+        assert want in taken, want
+    assert (96, 1) not in taken and (4, 3) not in taken
+
+
 def test_kernel_selection_and_strided(cuda):
     rng = np.random.default_rng(3)
     # rowdot: q = pi_1 (inner == 1), small m
     cases = [([64, 32, 16], [1, 2, 3], 1, 4, "rowdot"),
              ([64, 32, 16], [1, 2, 3], 2, 8, "colvec"),
+             ([256, 64, 512], [1, 2, 3], 2, 8, "stream_cols"),
+             ([257, 64, 512], [1, 2, 3], 2, 8, "colvec"),
              ([64, 32, 16], [1, 2, 3], 2, 40, "simt_gemm"),
              ([64, 32, 16], [2, 3, 1], 2, 40, "simt_gemm")]
     for na, pia, q, m, kern in cases:
@@ -133,7 +182,8 @@ def test_kernel_selection_and_strided(cuda):
                   wc=ka.dense_strides(nc, pia))
         a = rng.standard_normal(int(np.prod(na)))
         b = rng.standard_normal(m * nq)
-        c = abi_host(q, a, md, b)
+        # device operands: host ones above 64 MB are staged in pieces, which changes the choice
+        c = abi_device(q, a, md, b, cuda)
         assert _lib.last_kernel() == kern
         A = np.lib.stride_tricks.as_strided(a, shape=na, strides=[8 * w for w in md["wa"]])
         Bm = b.reshape(nq, m).T

@@ -79,7 +79,7 @@ def test_schedules_through_the_c_abi_agree(cuda):
     from ttm_b200.selector import Autotuner, valid_mask
     pr = dict(p=3, na=[64, 48, 40], q=2, pia=[1, 2, 3], m=8)
     ok = valid_mask(pr)
-    assert ok == [True, True, True, False, False]
+    assert ok == [True, True, True, False, False, True]
     tuner = Autotuner(cap=1 << 20)
     t = tuner.times(pr)
     assert [x is not None for x in t] == ok and all(x > 0 for x in t if x is not None)
@@ -88,7 +88,7 @@ def test_schedules_through_the_c_abi_agree(cuda):
     A = torch.randn(math.prod(na), device=cuda)
     B = torch.randn(m * na[q - 1], device=cuda)
     outs = []
-    for s in (1, 2, 3):
+    for s in (1, 2, 3, 6):
         Cc = torch.full((math.prod(na) // na[q - 1] * m,), float("nan"), device=cuda)
         from ttm_b200.selector import lib, _dense
         nc = list(na)

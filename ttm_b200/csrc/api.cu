@@ -35,6 +35,7 @@ const char* kernel_name(int id)
     case K_TC_OZAKI: return "tc_ozaki";
     case K_SPLIT_B: return "split_b";
     case K_GROUPED: return "grouped";
+    case K_STREAM_COLS: return "stream_cols";
     default: return "";
     }
 }
@@ -193,6 +194,8 @@ int note_launch(cudaError_t e, int kid)
     return TLIBTTM_OK;
 }
 
+constexpr int64_t kStreamMinBytes = int64_t(64) << 20;
+
 // All operands are device memory: enqueue on stream s.
 int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
 {
@@ -208,6 +211,11 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
     v.c = x.c;
     if (v.m <= kSmallM) {
         if (v.inner == 1) return note_launch(launch_rowdot(v, x.dtype, s), K_ROWDOT);
+        // The TMA-fed kernel wins once A streams from HBM; below about half of L2 the plain
+        // column kernel's shorter start-up wins (both measured on L2-resident repeats).
+        const int64_t a_bytes = v.outer * v.nq * v.inner * (x.dtype == TLIBTTM_F32 ? 4 : 8);
+        if (a_bytes >= kStreamMinBytes && stream_supported(v, x.dtype))
+            return note_launch(launch_stream(v, x.dtype, s), K_STREAM_COLS);
         return note_launch(launch_colvec(v, x.dtype, s), K_COLVEC);
     }
     if (precision == TLIBTTM_PREC_DEFAULT) precision = g_precision.load();
@@ -626,6 +634,7 @@ static bool sched_valid_view(int dtype, int schedule, const View3& v)
     case TLIBTTM_SCHED_COLS_SPLIT: return v.m <= kSmallM && v.inner >= 2;
     case TLIBTTM_SCHED_ROWS: return v.m <= kSmallM && v.inner == 1;
     case TLIBTTM_SCHED_TC_BF16X3: return dtype == TLIBTTM_F32 && tc_supported(v, TLIBTTM_PREC_BF16X3);
+    case TLIBTTM_SCHED_COLS_TMA: return stream_supported(v, dtype);
     default: return false;
     }
 }
@@ -662,6 +671,7 @@ int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p, const voi
     case TLIBTTM_SCHED_COLS: return note_launch(launch_colvec_ls(v, dtype, 1, s), K_COLVEC);
     case TLIBTTM_SCHED_COLS_SPLIT: return note_launch(launch_colvec_ls(v, dtype, 8, s), K_COLVEC);
     case TLIBTTM_SCHED_ROWS: return note_launch(launch_rowdot(v, dtype, s), K_ROWDOT);
+    case TLIBTTM_SCHED_COLS_TMA: return note_launch(launch_stream(v, dtype, s), K_STREAM_COLS);
     default: {
         int kid = K_NONE;
         e = launch_tc(v, TLIBTTM_PREC_BF16X3, s, &kid);

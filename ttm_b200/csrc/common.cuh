@@ -72,6 +72,7 @@ enum KernelId : int {
     K_TC_OZAKI,
     K_SPLIT_B,
     K_GROUPED,
+    K_STREAM_COLS,
     K_COUNT
 };
 

@@ -26,6 +26,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -113,6 +114,15 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
         ::"r"(su32(dst)), "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];"
+        ::"r"(su32(dst)), "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
 }
 
@@ -616,6 +626,254 @@ __global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m,
     }
 }
 
+// ------------------------------------------------------------------ TMA-fed small-m kernel
+// Exact (FMA in the I/O type) small-m contraction for strided fibres. A producer warp streams
+// 16 KB boxes of A into a ring with TMA; 8 consumer warps multiply them with B staged in shared
+// memory. A box holds P = 256 * W fibre positions x LB l, where W = 16 bytes / element size is
+// the number of consecutive positions one consumer thread owns (one 128-bit shared-memory read
+// per l, reused across all m rows of B). The positions are KB consecutive slices k of H * IB
+// consecutive i: with H = 1 the tensor map is (i, k, l) and IB a power of two covering inner
+// with little waste, so small inner extents still fill whole boxes; with H > 1 (few slices of
+// a large inner that IB divides) it is the 4D (i mod IB, i / IB, k, l). The dimensions are
+// deliberately not in stride order: either way a box lands in shared memory as
+// [l][P positions], position = (k * H + h) * IB + i mod IB.
+// Work unit = (tile, l range). When there are too few tiles to fill the GPU, or B is too large
+// to stage whole, the l range is split S ways: each unit stages only its rows of B, writes a
+// partial tile to a workspace, and the last unit of a tile to finish (atomic counter) adds the
+// S partials in a fixed order and stores C, so results do not depend on scheduling.
+constexpr int kStreamMaxStages = 8;
+constexpr int kStreamThreads = 9 * 32;          // 8 consumer warps + 1 producer warp
+constexpr uint32_t kStreamBox = 16384;          // bytes per box
+
+struct StreamParams {
+    const void* b;
+    void* c;
+    void* ws;               // S > 1: partial tiles [tiles][S][MB][P]
+    unsigned* cnt;          // S > 1: per-tile arrival counters, zero at launch
+    int* status;
+    int64_t outer, nq, inner, m;
+    int64_t tiles;          // ceil(outer / KB) * mper
+    int64_t mper;           // ceil(inner / IB)
+    int64_t units;          // tiles * S
+    int kchunks;            // ceil(nq / LB)
+    int kper;               // l chunks per unit
+    int S;                  // l ranges per tile
+    int b_cm;
+    int stages;             // ring depth, <= kStreamMaxStages
+    int ib_shift;           // log2(IB)
+    int h_shift;            // log2(H); H > 1 uses the 4D map
+    int kb;                 // KB = P / (IB * H)
+};
+
+template <typename T> struct V16Tc;
+template <> struct V16Tc<float> { using type = float4; };
+template <> struct V16Tc<double> { using type = double2; };
+
+template <typename T>
+struct StreamGeom {
+    static constexpr int W = 16 / (int)sizeof(T);                      // positions per thread
+    static constexpr int P = 256 * W;                                  // positions per box
+    static constexpr int LB = (int)(kStreamBox / (P * sizeof(T)));     // l per box (4)
+};
+
+template <typename T, int MB>
+__global__ void __maxnreg__(112)
+    stream_cols_kernel(const __grid_constant__ CUtensorMap amap, StreamParams P)
+{
+    using G = StreamGeom<T>;
+    constexpr int W = G::W, NP = G::P, LB = G::LB;
+    using V = typename V16Tc<T>::type;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int stages = P.stages;
+    uint8_t* ring = smem;
+    T* bs = reinterpret_cast<T*>(smem + stages * kStreamBox);                  // [kper * LB][MB]
+    uint64_t* full = reinterpret_cast<uint64_t*>(bs + (size_t)P.kper * LB * MB);
+    full = reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(full) + 15) & ~uintptr_t(15));
+    uint64_t* empty = full + kStreamMaxStages;
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + kStreamMaxStages);
+    volatile int* last_flag = abort_flag + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 8);
+        }
+        *abort_flag = 0;
+        *last_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int64_t mper = P.mper;
+    const int S = P.S;
+    const int IB = 1 << P.ib_shift;
+    if (warp == 8) {
+        if (lane == 0) {
+            int s = 0;
+            uint32_t ph = 0;
+            bool ok = true;
+            int issued[kStreamMaxStages];
+            for (int i = 0; i < kStreamMaxStages; ++i) issued[i] = -1;
+            for (int64_t u = blockIdx.x; u < P.units && ok; u += gridDim.x) {
+                const int64_t t = u / S;
+                const int r = (int)(u - t * S);
+                const int64_t kb = t / mper, ib = t - kb * mper;
+                const int kc0 = r * P.kper, kc1 = min(kc0 + P.kper, P.kchunks);
+                for (int kc = kc0; kc < kc1; ++kc) {
+                    if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    issued[s] = (int)ph;
+                    mbar_expect_tx(&full[s], kStreamBox);
+                    if (P.h_shift == 0)
+                        tma_load_3d(ring + s * kStreamBox, &amap, &full[s], (int)(ib * IB), (int)(kb * P.kb), kc * LB);
+                    else
+                        tma_load_4d(ring + s * kStreamBox, &amap, &full[s], 0, (int)(ib << P.h_shift), (int)(kb * P.kb),
+                                    kc * LB);
+                    if (++s == stages) { s = 0; ph ^= 1; }
+                }
+            }
+            for (int i = 0; i < stages; ++i) {
+                if (issued[i] < 0) continue;
+                const unsigned long long t0 = gtimer();
+                while (!mbar_try(&full[i], (uint32_t)issued[i]) && gtimer() - t0 < kTimeoutNs) {}
+            }
+        }
+    } else {
+        const int tid = threadIdx.x;                       // 0..255
+        const int pos = tid * W;                           // first owned position
+        const int kk = pos >> (P.ib_shift + P.h_shift);
+        const int hh = (pos >> P.ib_shift) & ((1 << P.h_shift) - 1), ii = pos & (IB - 1);
+        const T* Bg = static_cast<const T*>(P.b);
+        T* C = static_cast<T*>(P.c);
+        int s = 0;
+        uint32_t ph = 0;
+        bool ok = true;
+        int staged = -1;                                   // l range (r) held in bs
+        // Every consumer runs every iteration and meets the consumer barriers the same number of
+        // times; after an abort the waits are skipped and no work is done.
+        for (int64_t u = blockIdx.x; u < P.units; u += gridDim.x) {
+            const int64_t t = u / S;
+            const int r = (int)(u - t * S);
+            const int64_t kb = t / mper, ib = t - kb * mper;
+            const int kc0 = r * P.kper, kc1 = min(kc0 + P.kper, P.kchunks);
+            if (r != staged) {
+                // stage rows [kc0 * LB, kc1 * LB) of B: bs[l][j] = B(j, l), zero outside B
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+                const int rows = (kc1 - kc0) * LB;
+                for (int e = tid; e < rows * MB; e += 256) {
+                    const int lr = e / MB, j = e - lr * MB;
+                    const int64_t l = (int64_t)kc0 * LB + lr;
+                    bs[e] = (j < P.m && l < P.nq) ? (P.b_cm ? Bg[j + l * P.m] : Bg[j * P.nq + l]) : T(0);
+                }
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+                staged = r;
+            }
+            T acc[W][MB];
+#pragma unroll
+            for (int w = 0; w < W; ++w)
+#pragma unroll
+                for (int j = 0; j < MB; ++j) acc[w][j] = T(0);
+            for (int kc = kc0; kc < kc1; ++kc) {
+                const bool got = ok && mbar_wait(&full[s], ph, abort_flag);
+                const bool have = __all_sync(0xffffffffu, got);
+                if (!have) ok = false;
+                if (have) {
+                    const V* box = reinterpret_cast<const V*>(ring + s * kStreamBox) + tid;
+                    const T* brow = bs + (size_t)(kc - kc0) * LB * MB;
+                    // all LB reads up front, except at MB = 16 where the registers go to acc
+                    constexpr int PRE = MB < 16 ? LB : 1;
+                    V av[PRE];
+#pragma unroll
+                    for (int l = 0; l < PRE; ++l) av[l] = box[l * (NP / W)];
+#pragma unroll
+                    for (int l = 0; l < LB; ++l) {
+                        V a1;
+                        if constexpr (PRE == 1) a1 = l == 0 ? av[0] : box[l * (NP / W)];
+                        else a1 = av[l];
+                        const T* a = reinterpret_cast<const T*>(&a1);
+                        const T* bl = brow + l * MB;
+                        if constexpr (MB % W == 0) {
+#pragma unroll
+                            for (int c = 0; c < MB / W; ++c) {
+                                const V bv = *reinterpret_cast<const V*>(bl + c * W);
+                                const T* b = reinterpret_cast<const T*>(&bv);
+#pragma unroll
+                                for (int e = 0; e < W; ++e)
+#pragma unroll
+                                    for (int w = 0; w < W; ++w) acc[w][c * W + e] = fma(a[w], b[e], acc[w][c * W + e]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < MB; ++j) {
+                                const T b = bl[j];
+#pragma unroll
+                                for (int w = 0; w < W; ++w) acc[w][j] = fma(a[w], b, acc[w][j]);
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s]);
+                }
+                if (++s == stages) { s = 0; ph ^= 1; }
+            }
+            const int64_t k = kb * P.kb + kk, i = (((ib << P.h_shift) + hh) << P.ib_shift) + ii;
+            const bool mine = k < P.outer && i < P.inner;     // all W positions share k; inner % W == 0
+            if (S == 1) {
+                if (ok && mine) {
+                    T* cp = C + (k * P.m) * P.inner + i;
+#pragma unroll
+                    for (int j = 0; j < MB; ++j) {
+                        if (j < P.m) {
+                            V v;
+                            T* vv = reinterpret_cast<T*>(&v);
+#pragma unroll
+                            for (int w = 0; w < W; ++w) vv[w] = acc[w][j];
+                            *reinterpret_cast<V*>(cp + (int64_t)j * P.inner) = v;
+                        }
+                    }
+                }
+            } else {
+                T* wsp = static_cast<T*>(P.ws) + ((size_t)u * MB) * NP + pos;
+#pragma unroll
+                for (int j = 0; j < MB; ++j) {
+                    V v;
+                    T* vv = reinterpret_cast<T*>(&v);
+#pragma unroll
+                    for (int w = 0; w < W; ++w) vv[w] = acc[w][j];
+                    *reinterpret_cast<V*>(wsp + (size_t)j * NP) = v;
+                }
+                __threadfence();
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+                if (tid == 0) *last_flag = (!*abort_flag && atomicAdd(&P.cnt[t], 1u) == (unsigned)(S - 1)) ? 1 : 0;
+                asm volatile("bar.sync 1, 256;" ::: "memory");
+                if (*last_flag) {
+                    __threadfence();
+                    if (mine) {
+                        const T* w0 = static_cast<const T*>(P.ws) + ((size_t)t * S * MB) * NP + pos;
+                        T* cp = C + (k * P.m) * P.inner + i;
+                        for (int j = 0; j < MB && j < P.m; ++j) {
+                            V sum;
+                            T* sv = reinterpret_cast<T*>(&sum);
+#pragma unroll
+                            for (int w = 0; w < W; ++w) sv[w] = T(0);
+                            for (int rr = 0; rr < S; ++rr) {
+                                const V v = __ldcg(reinterpret_cast<const V*>(w0 + ((size_t)rr * MB + j) * NP));
+                                const T* vv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+                                for (int w = 0; w < W; ++w) sv[w] += vv[w];
+                            }
+                            *reinterpret_cast<V*>(cp + (int64_t)j * P.inner) = sum;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(P.status, 1);
+}
+
 // ------------------------------------------------------------------ host side
 // Per-device state: the device status word that kernels raise on a failed bounded wait.
 struct DevState {
@@ -775,7 +1033,245 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
+// A as a tensor map over (i, k, l), or with h > 1 over (i mod ib, i / ib, k, l) (ib must divide
+// inner) -- dimensions deliberately not in stride order -- with boxes of ib x [h x] kb x LB.
+bool encode_stream_map(const View3& v, int dtype, int ib, int h, int kb, CUtensorMap* map)
+{
+    EncodeTiledFn cuTensorMapEncodeTiled = encode_fn();
+    if (!cuTensorMapEncodeTiled) return false;
+    const size_t es = dtype == 0 ? 4 : 8;
+    const cuuint32_t lb = dtype == 0 ? (cuuint32_t)StreamGeom<float>::LB : (cuuint32_t)StreamGeom<double>::LB;
+    const CUtensorMapDataType ty = dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUresult r;
+    if (h <= 1) {
+        cuuint64_t dims[3] = {(cuuint64_t)v.inner, (cuuint64_t)v.outer, (cuuint64_t)v.nq};
+        cuuint64_t strides[2] = {(cuuint64_t)(v.inner * v.nq) * es, (cuuint64_t)v.inner * es};
+        cuuint32_t box[3] = {(cuuint32_t)ib, (cuuint32_t)kb, lb};
+        cuuint32_t el[3] = {1, 1, 1};
+        r = cuTensorMapEncodeTiled(map, ty, 3, const_cast<void*>(v.a), dims, strides, box, el,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    } else {
+        if (v.inner % ib != 0) return false;
+        cuuint64_t dims[4] = {(cuuint64_t)ib, (cuuint64_t)(v.inner / ib), (cuuint64_t)v.outer, (cuuint64_t)v.nq};
+        cuuint64_t strides[3] = {(cuuint64_t)ib * es, (cuuint64_t)(v.inner * v.nq) * es, (cuuint64_t)v.inner * es};
+        cuuint32_t box[4] = {(cuuint32_t)ib, (cuuint32_t)h, (cuuint32_t)kb, lb};
+        cuuint32_t el[4] = {1, 1, 1, 1};
+        r = cuTensorMapEncodeTiled(map, ty, 4, const_cast<void*>(v.a), dims, strides, box, el,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+    return r == CUDA_SUCCESS;
+}
+
+// cudaFuncSetAttribute once per kernel instance and device (devices 0..63).
+template <typename K>
+cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done)
+{
+    const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
+
+template <typename T, int MB>
+cudaError_t launch_stream_mb(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
+                             cudaStream_t s)
+{
+    static std::atomic<uint64_t> done{0};
+    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB>, dev, done);
+    if (e != cudaSuccess) return e;
+    stream_cols_kernel<T, MB><<<grid, kStreamThreads, smem, s>>>(amap, P);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_stream_t(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
+                            cudaStream_t s)
+{
+    if (P.m <= 1) return launch_stream_mb<T, 1>(amap, P, smem, grid, dev, s);
+    if (P.m <= 2) return launch_stream_mb<T, 2>(amap, P, smem, grid, dev, s);
+    if (P.m <= 4) return launch_stream_mb<T, 4>(amap, P, smem, grid, dev, s);
+    if (P.m <= 8) return launch_stream_mb<T, 8>(amap, P, smem, grid, dev, s);
+    return launch_stream_mb<T, 16>(amap, P, smem, grid, dev, s);
+}
+
+// Launch geometry of the TMA-fed small-m kernel (two CTAs per SM): box shape, ring depth, the
+// l split and the dynamic shared memory (ring + staged rows of B + barriers).
+struct StreamShape {
+    int ib, ib_shift, h_shift, kb, kchunks, kper, S, stages, mb;
+    int64_t tiles, mper, units;
+    size_t smem, ws_bytes;
+};
+
+bool stream_shape(const View3& v, int dtype, int sms, StreamShape& sh)
+{
+    const size_t es = dtype == 0 ? 4 : 8;
+    const int W = 16 / (int)es, NP = 256 * W, LB = (int)(kStreamBox / (NP * es));
+    sh.mb = v.m <= 1 ? 1 : v.m <= 2 ? 2 : v.m <= 4 ? 4 : v.m <= 8 ? 8 : 16;
+    // Box shape: among the shapes whose boxes are at most 20% out-of-range fill (positions past
+    // inner or outer), the one with the fewest positions, where rows under 32 bytes count
+    // double (they use half of each DRAM sector they touch). Candidates: (IB, H = 1) with IB a
+    // power of two in [W, 256] (so KB = NP / IB <= 256), and the folded (IB, H > 1) with IB the
+    // largest power of two (<= 256, rows >= 128 bytes) dividing inner. None: not supported.
+    const int64_t valid = v.inner * v.outer;
+    int64_t best_cost = -1;
+    auto consider = [&](int ibs, int hs, int64_t tiles, bool narrow) {
+        const int64_t pos = tiles * NP;
+        if (pos * 4 > valid * 5) return;
+        const int64_t cost = narrow ? 2 * pos : pos;
+        if (best_cost < 0 || cost < best_cost || (cost == best_cost && hs == 0 && ibs > sh.ib_shift)) {
+            best_cost = cost;
+            sh.ib_shift = ibs;
+            sh.h_shift = hs;
+        }
+    };
+    for (int ibs = 0; (1 << ibs) <= 256; ++ibs) {
+        const int64_t ib = int64_t(1) << ibs;
+        if (ib < W) continue;
+        const int64_t kb = NP / ib;
+        consider(ibs, 0, ((v.inner + ib - 1) / ib) * ((v.outer + kb - 1) / kb), ib * (int64_t)es < 32 && ib < v.inner);
+    }
+    int fb = 0;
+    while (fb < 8 && v.inner % (int64_t(1) << (fb + 1)) == 0) ++fb;
+    if ((int64_t(1) << fb) * (int64_t)es >= 128) {
+        const int64_t ib = int64_t(1) << fb, nhi = v.inner / ib;
+        for (int hs = 1; (ib << hs) <= NP; ++hs) {
+            const int64_t h = int64_t(1) << hs, kb = NP / (ib * h);
+            consider(fb, hs, ((nhi + h - 1) / h) * ((v.outer + kb - 1) / kb), false);
+        }
+    }
+    if (best_cost < 0) return false;
+    sh.ib = 1 << sh.ib_shift;
+    sh.kb = NP / (sh.ib << sh.h_shift);
+    sh.mper = sh.h_shift ? ((v.inner >> sh.ib_shift) + (1 << sh.h_shift) - 1) >> sh.h_shift
+                         : (v.inner + sh.ib - 1) / sh.ib;
+    sh.tiles = ((v.outer + sh.kb - 1) / sh.kb) * sh.mper;
+    sh.kchunks = (int)((v.nq + LB - 1) / LB);
+    const size_t budget = 112 * 1024 - 1024 - 256;   // per CTA, two per SM
+    const size_t row = (size_t)LB * sh.mb * es;      // staged B bytes per l chunk
+    int kper_max = 0;
+    sh.stages = 0;
+    for (int st = 6; st >= 4; --st)
+        if ((size_t)sh.kchunks * row <= budget - (size_t)st * kStreamBox) {
+            sh.stages = st;
+            kper_max = sh.kchunks;
+            break;
+        }
+    if (!sh.stages) {
+        sh.stages = 5;
+        kper_max = (int)((budget - 5 * (size_t)kStreamBox) / row);
+    }
+    // l split: the S (at least enough for B to fit) with the shortest estimated makespan, in
+    // boxes: rounds of units over the CTA slots x (boxes per unit + 1 for the pipeline ramp
+    // + 3 + MB / 2 for writing, fencing and re-reading a partial tile when S > 1); a split must
+    // win by 10% (measured: splits cost more than this model says)
+    const int64_t slots = 2 * (int64_t)sms;
+    const int64_t s_min = (sh.kchunks + kper_max - 1) / kper_max;
+    const int64_t s_max = std::max<int64_t>(s_min, std::min<int64_t>(sh.kchunks, 64));
+    double best_t = 0;
+    sh.kper = sh.kchunks;
+    for (int64_t S = s_min; S <= s_max; ++S) {
+        const int64_t kper = (sh.kchunks + S - 1) / S;
+        if (kper > kper_max) continue;
+        const int64_t s_eff = (sh.kchunks + kper - 1) / kper;
+        const int64_t rounds = (sh.tiles * s_eff + slots - 1) / slots;
+        const double t = (double)rounds * ((double)kper + 1.0 + (s_eff > 1 ? 3.0 + sh.mb / 2.0 : 0.0));
+        if (S == s_min || t < best_t * 0.9) { best_t = t; sh.kper = (int)kper; }
+    }
+    sh.S = (sh.kchunks + sh.kper - 1) / sh.kper;
+    sh.units = sh.tiles * sh.S;
+    sh.smem = 1024 + (size_t)sh.stages * kStreamBox + (size_t)sh.kper * row + 256;
+    sh.ws_bytes = sh.S > 1 ? (size_t)sh.units * sh.mb * NP * es : 0;
+    return true;
+}
+
 }  // namespace
+
+// Whether the driver accepts tensor maps whose dimensions are not in stride order (checked once,
+// on a dummy address: encoding reads no memory).
+bool permuted_maps_ok()
+{
+    static bool ok = false;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        alignas(16) static const double probe[4] = {0, 0, 0, 0};
+        View3 v{};
+        v.a = probe;
+        v.inner = 4;
+        v.outer = 3;
+        v.nq = 5;
+        CUtensorMap map;
+        ok = encode_stream_map(v, 0, 4, 1, 256, &map) && encode_stream_map(v, 1, 4, 1, 128, &map);
+        v.inner = 256;
+        ok = ok && encode_stream_map(v, 0, 32, 4, 8, &map) && encode_stream_map(v, 1, 16, 4, 8, &map);
+    });
+    return ok;
+}
+
+bool stream_supported(const View3& v, int dtype)
+{
+    if (!permuted_maps_ok()) return false;
+    // 16-byte rows and 16-byte vectors of W consecutive positions in A and C
+    const int64_t w = dtype == 0 ? 4 : 2;
+    if (v.m > kSmallM || v.inner < w || v.inner % w != 0) return false;
+    if (((reinterpret_cast<uintptr_t>(v.a) | reinterpret_cast<uintptr_t>(v.c)) & 15u) != 0) return false;
+    if (v.outer >= (int64_t(1) << 31) || v.nq >= (int64_t(1) << 31) || v.inner >= (int64_t(1) << 31)) return false;
+    // shapes whose boxes would be mostly out-of-range fill go elsewhere
+    StreamShape sh;
+    return stream_shape(v, dtype, 148, sh);
+}
+
+cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (!g_sm_count) {
+        e = cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    DevState* st = nullptr;
+    if ((e = state_for(dev, st)) != cudaSuccess) return e;
+    StreamShape sh;
+    if (!stream_shape(v, dtype, g_sm_count, sh)) return cudaErrorNotSupported;
+    CUtensorMap amap;
+    if (!encode_stream_map(v, dtype, sh.ib, 1 << sh.h_shift, sh.kb, &amap)) return cudaErrorInvalidValue;
+    StreamParams P{};
+    P.b = v.b;
+    P.c = v.c;
+    P.status = st->status;
+    P.outer = v.outer;
+    P.nq = v.nq;
+    P.inner = v.inner;
+    P.m = v.m;
+    P.tiles = sh.tiles;
+    P.mper = sh.mper;
+    P.units = sh.units;
+    P.kchunks = sh.kchunks;
+    P.kper = sh.kper;
+    P.S = sh.S;
+    P.b_cm = v.b_cm;
+    P.stages = sh.stages;
+    P.ib_shift = sh.ib_shift;
+    P.h_shift = sh.h_shift;
+    P.kb = sh.kb;
+    void* scratch = nullptr;
+    if (sh.S > 1) {
+        const size_t ws = (sh.ws_bytes + 255) & ~size_t(255);
+        if ((e = cudaMallocAsync(&scratch, ws + (size_t)sh.tiles * sizeof(unsigned), s)) != cudaSuccess) return e;
+        P.ws = scratch;
+        P.cnt = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(scratch) + ws);
+        e = cudaMemsetAsync(P.cnt, 0, (size_t)sh.tiles * sizeof(unsigned), s);
+    }
+    const int grid = (int)std::min<int64_t>(sh.units, (int64_t)g_sm_count * 2);
+    if (e == cudaSuccess)
+        e = dtype == 0 ? launch_stream_t<float>(amap, P, sh.smem, grid, dev, s)
+                       : launch_stream_t<double>(amap, P, sh.smem, grid, dev, s);
+    if (scratch) cudaFreeAsync(scratch, s);
+    return e;
+}
 
 bool tc_supported(const View3& v, int precision)
 {

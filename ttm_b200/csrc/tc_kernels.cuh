@@ -16,6 +16,10 @@ cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid);
 // capture does not need to allocate it).
 cudaError_t tc_prepare_device();
 
+// TMA-fed exact small-m kernel for strided fibres (inner % 4 == 0, m <= 16, B fits shared memory).
+bool stream_supported(const View3& v, int dtype);
+cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s);
+
 // Frees device state owned by the tensor-core paths on the current device.
 void tc_release_buffers();
 

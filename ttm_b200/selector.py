@@ -33,8 +33,9 @@ try:
 except Exception:  # noqa: BLE001
     torch = None
 
-SCHEDULES = ["simt_gemm", "cols", "cols_split", "rows", "tc_bf16x3"]   # ids 1..5 of tlibttm_schedule
-EXACT = [1, 2, 3, 4]                  # schedules that compute with exact FMA in the I/O type
+SCHEDULES = ["simt_gemm", "cols", "cols_split", "rows", "tc_bf16x3", "cols_tma"]   # ids 1..6 of tlibttm_schedule
+EXACT = [1, 2, 3, 4, 6]               # schedules that compute with exact FMA in the I/O type
+NS = len(SCHEDULES)
 FEATURES = 53
 HIDDEN = 64
 MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "schedule_model.json")
@@ -98,7 +99,7 @@ def features(pr, dtype_id=_lib.F32):
 def valid_mask(pr, dtype_id=_lib.F32):
     L = lib()
     na, pia = _lib.sz(pr["na"]), _lib.sz(pr["pia"])
-    return [bool(L.tlibttm_schedule_valid(dtype_id, s, pr["q"], pr["p"], na, pia, pr["m"])) for s in range(1, 6)]
+    return [bool(L.tlibttm_schedule_valid(dtype_id, s, pr["q"], pr["p"], na, pia, pr["m"])) for s in range(1, NS + 1)]
 
 
 # ------------------------------------------------------------------------------ autotuner
@@ -128,7 +129,7 @@ class Autotuner:
         _lib.check(rc)
 
     def times(self, pr):
-        """Median run time in microseconds per schedule 1..5 (None where invalid)."""
+        """Median run time in microseconds per schedule 1..NS (None where invalid)."""
         k = self.key(pr)
         if k in self.db:
             return self.db[k]
@@ -140,7 +141,7 @@ class Autotuner:
         md = [_lib.sz(na), _lib.sz(wa), _lib.sz(pia), _lib.sz([m, na[q - 1]]), _lib.sz([1, 2]), _lib.sz(nc),
               _lib.sz(wc)]
         out = []
-        for s, ok in zip(range(1, 6), valid_mask(pr, self.dtype_id)):
+        for s, ok in zip(range(1, NS + 1), valid_mask(pr, self.dtype_id)):
             if not ok:
                 out.append(None)
                 continue
@@ -157,7 +158,7 @@ class Autotuner:
 
     def best(self, pr, allowed=None):
         t = self.times(pr)
-        cands = [(t[s - 1], s) for s in range(1, 6) if t[s - 1] is not None and (allowed is None or s in allowed)]
+        cands = [(t[s - 1], s) for s in range(1, NS + 1) if t[s - 1] is not None and (allowed is None or s in allowed)]
         return min(cands)[1]
 
 
@@ -269,7 +270,10 @@ class Selector:
 
     def choose(self, pr, allowed, dtype_id=_lib.F32):
         ok = valid_mask(pr, dtype_id)
-        cands = [s for s in range(1, 6) if ok[s - 1] and s in allowed]
+        # a model trained before a schedule existed never proposes it
+        cands = [s for s in range(1, NS + 1) if ok[s - 1] and s in allowed and s <= self.model.dims[-1]]
+        if not cands:
+            raise ValueError("no allowed schedule can run this problem")
         if len(cands) == 1:
             return cands[0], False
         X = torch.tensor([features(pr, dtype_id)], device=self.model.device)
@@ -318,7 +322,7 @@ def train_and_evaluate(n_train, n_test, steps=3000, seed_train=1, seed_test=2, m
     log(f"timed {n_train} training problems in {time.time() - t0:.0f} s")
     model = MLP().fit(X, T, M, steps=steps, log=log)
     dataset(tuner, test)
-    allowed_sets = {"exact": set(EXACT), "fp32_accurate": {1, 2, 3, 4, 5}}
+    allowed_sets = {"exact": set(EXACT), "fp32_accurate": set(range(1, NS + 1))}
     out = {"n_train": n_train, "n_test": n_test, "steps": steps, "margin": margin}
     for name, allowed in allowed_sets.items():
         sel = Selector(model, tuner, margin=margin)
@@ -348,6 +352,8 @@ def _heuristic_in(pr, allowed):
     if pr["m"] <= 16:
         if inner == 1:
             return 4
+        if 6 in allowed and math.prod(pr["na"]) * 4 >= 64 << 20 and valid_mask(pr)[5]:
+            return 6
         rv = 4
         w = rv if inner % rv == 0 else 1
         return 3 if math.ceil(inner * outer / (32 * w)) < 148 * 32 else 2

@@ -144,7 +144,7 @@ def _ttm_torch(q, A, B, precision):
         # the learned schedule selector picks among the exact kernels (float32 may also take bf16x3)
         from . import selector
         pr = dict(p=p, na=na, q=q, pia=pia, m=nb[0])
-        allowed = {1, 2, 3, 4, 5} if A.dtype == torch.float32 else {1, 2, 3, 4}
+        allowed = set(range(1, selector.NS + 1)) if A.dtype == torch.float32 else set(selector.EXACT)
         with torch.cuda.device(A.device):
             sched, _ = selector.default_selector(A.device).choose(pr, allowed, _dtype_id(A.dtype))
             _lib.check(selector.lib().tlibttm_ttm_sched(_dtype_id(A.dtype), sched, q, p, A.data_ptr(), _lib.sz(na),
