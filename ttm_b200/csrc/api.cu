@@ -19,6 +19,7 @@
 #include "tlib/detail/strides.h"
 
 #include "common.cuh"
+#include "tc8_kernels.cuh"
 #include "tc_kernels.cuh"
 
 namespace tlibttm {
@@ -228,6 +229,12 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
     }
     if (precision == TLIBTTM_PREC_OZAKI && x.dtype != TLIBTTM_F64)
         return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm: the ozaki precision takes double operands.");
+    if ((precision == TLIBTTM_PREC_FP8 || precision == TLIBTTM_PREC_OZAKI) && tc8_supported(v, precision, x.dtype)) {
+        int kid = K_NONE, n = 0;
+        cudaError_t e = launch_tc8(v, precision, x.dtype, s, &kid, &n);
+        if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);   // exponent and slicer kernels
+        return note_launch(e, kid);
+    }
     if (precision != TLIBTTM_PREC_PLAIN && tc_supported(v, precision)) {
         int kid = K_NONE;
         cudaError_t e = launch_tc(v, precision, s, &kid);

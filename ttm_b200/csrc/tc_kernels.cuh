@@ -26,6 +26,9 @@ void tc_release_buffers();
 // Reads and clears the device status word (non-zero: a kernel gave up on a bounded wait).
 int tc_read_status();
 
+// The device status word of device `dev` (created on first use), for kernels in other files.
+cudaError_t tc_status_word(int dev, int** out);
+
 // Largest pre-split B image the allocation-free bf16x3 variant can hold (bytes):
 // ceil(m/16)*16 * ceil(n_q/16)*16 * 4 <= 1 MiB for m <= 256, e.g. m = 256 with n_q <= 1024.
 constexpr size_t kNoAllocImageBytes = size_t(1) << 20;
