@@ -313,7 +313,7 @@ def run_ours(args):
         C4 = C.view(S, S, S, S)
         Bq = Bs[q - 1].view(S, S).double().cpu().numpy()   # [l][j] : column-major (m, nq)
         num = den = 0.0
-        worst = 0.0
+        dmax = rmax = 0.0
         for _ in range(24):
             idx = [int(x) for x in rng.integers(0, S, size=4)]
             sl = [slice(None) if (3 - d) == (q - 1) else idx[d] for d in range(4)]
@@ -322,8 +322,9 @@ def run_ours(args):
             want = fib @ Bq
             num += float(np.sum((got - want) ** 2))
             den += float(np.sum(want ** 2))
-            worst = max(worst, float(np.max(np.abs(got - want) / np.maximum(np.abs(want), 1e-30))))
-        relerr[q] = (float(np.sqrt(num / den)), worst)
+            dmax = max(dmax, float(np.max(np.abs(got - want))))
+            rmax = max(rmax, float(np.max(np.abs(want))))
+        relerr[q] = (float(np.sqrt(num / den)), dmax / rmax)
     kernel_name = _lib.last_kernel()
 
     for _ in range(max(3, args.warmup)):
@@ -419,6 +420,8 @@ def run_ours(args):
                        "flop_per_step": flops_per_step(S), "parallelism": f"replicas x{world} (one per GPU)",
                        "l2": "inputs (17.2 GB per tensor at S=256) exceed the 126 MB L2; no flush"},
             "rel_error_vs_fp64": {f"q{q}": {"fro": relerr[q][0], "max": relerr[q][1]} for q in relerr},
+            "rel_error_note": "24 sampled fibres per q vs float64 dot products: fro = ||c-r||/||r||, "
+                              "max = max|c-r|/max|r|",
             "plain_fp32_tflops": plain_tflops,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved_gbs / hbm_peak, "traffic": None, "peak_kind": peak_kind,

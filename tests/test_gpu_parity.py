@@ -131,7 +131,8 @@ def test_stream_cols_box_shapes(cuda, oracle_c, dtype):
     shapes = [(4, 300, 5, 1), (4, 1000, 70, 16), (8, 257, 33, 8), (12, 700, 16, 3), (36, 120, 9, 2),
               (64, 37, 33, 8), (64, 130, 1000, 1), (100, 256, 16, 4), (128, 37, 33, 8), (260, 256, 5, 1),
               (256, 4, 3000, 16), (512, 2, 1000, 1), (4096, 1, 37, 8), (1536, 2, 9, 2), (65536, 1, 3, 1),
-              (8192, 3, 20, 4), (96, 1, 50, 16), (4, 3, 16, 3)]
+              (8192, 3, 20, 4), (96, 1, 50, 16), (4, 3, 16, 3),
+              (64, 200, 1, 4), (4, 1000, 2, 8), (128, 40, 3, 16)]       # n_q below one box of l
     if dtype == np.float64:
         shapes += [(2, 512, 7, 2), (6, 256, 9, 8)]
     dt = _lib.F32 if dtype == np.float32 else _lib.F64
@@ -160,9 +161,30 @@ def test_stream_cols_box_shapes(cuda, oracle_c, dtype):
         oracle_c.ttm(2, a, na, md["wa"], pia, b, md["nb"], md["pib"], ref, nc, md["wc"])
         assert relerr(c, ref) <= (1e-14 if dtype == np.float64 else 2e-6), (inner, outer, nq, m)
     # the folded boxes, the restaged B and the narrow-row boxes were all exercised
-    for want in ((4096, 1), (65536, 1), (512, 2), (256, 4), (4, 1000)):
+    for want in ((4096, 1), (65536, 1), (512, 2), (256, 4), (4, 1000), (64, 200), (128, 40)):
         assert want in taken, want
     assert (96, 1) not in taken and (4, 3) not in taken
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_short_contiguous_fibres(cuda, oracle_c, dtype):
+    """q = pi_1 with n_q <= 16: rows of A are short and contiguous (the flat-tile row kernel);
+    row counts that are not multiples of a warp's tile, n_q = 1, every m bucket, both B layouts."""
+    rng = np.random.default_rng(31)
+    for n, (nq, outer, m) in enumerate(((1, 5000, 1), (2, 70001, 8), (3, 4099, 3), (5, 12345, 16), (16, 33333, 2),
+                                        (16, 31, 5), (7, 100000, 1))):
+        na = [nq, outer]
+        pia = [1, 2]
+        nc = [m, outer]
+        md = dict(na=na, wa=ka.dense_strides(na, pia), pia=pia, nb=[m, nq], pib=[1, 2] if n % 2 else [2, 1],
+                  nc=nc, wc=ka.dense_strides(nc, pia))
+        a = rng.standard_normal(nq * outer).astype(dtype)
+        b = rng.standard_normal(m * nq).astype(dtype)
+        c = abi_device(1, a, md, b, cuda)
+        assert _lib.last_kernel() == "rowdot"
+        ref = np.zeros(m * outer, dtype=dtype)
+        oracle_c.ttm(1, a, na, md["wa"], pia, b, md["nb"], md["pib"], ref, nc, md["wc"])
+        assert relerr(c, ref) <= (1e-14 if dtype == np.float64 else 2e-6), (nq, outer, m)
 
 
 def test_kernel_selection_and_strided(cuda):

@@ -14,6 +14,8 @@
 //  strided    definition-level kernel for non-dense (but valid) strides.
 //
 // All index arithmetic is 64-bit (a 256^4 tensor has 2^32 elements).
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace tlibttm {
@@ -480,6 +482,61 @@ __global__ void __launch_bounds__(256) rowdot_kernel(View3 v)
 }
 
 // ---------------------------------------------------------------------------------------------
+// rowflat: small m, contiguous fibres of at most kFlatMaxNq elements (inner == 1, short rows).
+// A warp's wr consecutive rows are wr * nq contiguous elements: the warp copies them with
+// coalesced loads into shared memory with rows padded to nq + 1 (conflict-free row reads), then
+// each lane computes every 32nd row. B sits in shared memory as bs[l][j].
+// ---------------------------------------------------------------------------------------------
+constexpr int kFlatMaxNq = 16;
+
+template <typename T, int MB>
+__global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
+{
+    constexpr int MBP = MB < 4 ? 4 : MB;
+    extern __shared__ __align__(16) unsigned char flat_raw[];
+    T* smf = reinterpret_cast<T*>(flat_raw);
+    const int nq = (int)v.nq, stride = nq + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    T* tile = smf + (size_t)warp * wr * stride;
+    T* bs = smf + (size_t)8 * wr * stride;
+    const T* __restrict__ B = static_cast<const T*>(v.b);
+    for (int e = threadIdx.x; e < nq * MBP; e += blockDim.x) {
+        const int l = e / MBP, j = e - l * MBP;
+        bs[e] = j < v.m ? (v.b_cm ? B[j + (int64_t)l * v.m] : B[(int64_t)j * nq + l]) : T(0);
+    }
+    __syncthreads();
+    const int64_t wrow0 = ((int64_t)blockIdx.x * 8 + warp) * wr;
+    if (wrow0 >= v.outer) return;
+    const int nrow = (int)((v.outer - wrow0) < wr ? (v.outer - wrow0) : wr);
+    const T* __restrict__ A = static_cast<const T*>(v.a) + wrow0 * nq;
+    const int cnt = nrow * nq;
+    // e / nq == umulhi(e, ceil(2^32 / nq)) for these e (nq > 1; 2^32 itself does not fit)
+    const uint32_t inv = nq > 1 ? (uint32_t)((0x100000000ull + nq - 1) / nq) : 0u;
+#pragma unroll 16
+    for (int e = lane; e < cnt; e += 32) {
+        const int r = nq > 1 ? (int)__umulhi((uint32_t)e, inv) : e;
+        tile[r * stride + (e - r * nq)] = __ldg(A + e);
+    }
+    __syncwarp();
+    T* __restrict__ Cp = static_cast<T*>(v.c);
+    for (int r = lane; r < nrow; r += 32) {
+        T acc[MB];
+#pragma unroll
+        for (int j = 0; j < MB; ++j) acc[j] = T(0);
+        const T* row = tile + r * stride;
+        for (int l = 0; l < nq; ++l) {
+            const T a = row[l];
+#pragma unroll
+            for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bs[l * MBP + j], acc[j]);
+        }
+        T* cp = Cp + (wrow0 + r) * v.m;
+#pragma unroll
+        for (int j = 0; j < MB; ++j)
+            if (j < v.m) cp[j] = acc[j];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // strided: one thread per C element, strides taken from the caller.
 // ---------------------------------------------------------------------------------------------
 template <typename T>
@@ -655,9 +712,30 @@ cudaError_t rowdot_dispatch_v(const View3& v, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <typename T, int MB>
+cudaError_t rowflat_launch(const View3& v, cudaStream_t s)
+{
+    // rows per warp: about 4 KB of A, a multiple of 32, with the block's tiles within 44 KB of
+    // shared memory (no opt-in needed)
+    const int64_t want = 4096 / (v.nq * (int64_t)sizeof(T));
+    const int64_t cap = (44 * 1024 - 16 * 16 * (int64_t)sizeof(T)) / (8 * (v.nq + 1) * (int64_t)sizeof(T));
+    const int wr = (int)std::max<int64_t>(32, std::min(want, cap) / 32 * 32);
+    const size_t smem = ((size_t)8 * wr * (v.nq + 1) + (size_t)v.nq * (MB < 4 ? 4 : MB)) * sizeof(T);
+    const int64_t blocks = ceil_div(v.outer, (int64_t)8 * wr);
+    rowflat_kernel<T, MB><<<(unsigned)blocks, 256, smem, s>>>(v, wr);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t rowdot_dispatch(const View3& v, cudaStream_t s)
 {
+    if (v.nq <= kFlatMaxNq) {
+        if (v.m <= 1) return rowflat_launch<T, 1>(v, s);
+        if (v.m <= 2) return rowflat_launch<T, 2>(v, s);
+        if (v.m <= 4) return rowflat_launch<T, 4>(v, s);
+        if (v.m <= 8) return rowflat_launch<T, 8>(v, s);
+        return rowflat_launch<T, 16>(v, s);
+    }
     constexpr int RV = 16 / sizeof(T);
     const bool vec = aligned16(v.a) && (v.nq % RV == 0);
     return vec ? rowdot_dispatch_v<T, true>(v, s) : rowdot_dispatch_v<T, false>(v, s);

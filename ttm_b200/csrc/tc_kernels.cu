@@ -484,9 +484,9 @@ __global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m,
 // ------------------------------------------------------------------ TMA-fed small-m kernel
 // Exact (FMA in the I/O type) small-m contraction for strided fibres. A producer warp streams
 // 16 KB boxes of A into a ring with TMA; 8 consumer warps multiply them with B staged in shared
-// memory. A box holds P = 256 * W fibre positions x LB l, where W = 16 bytes / element size is
-// the number of consecutive positions one consumer thread owns (one 128-bit shared-memory read
-// per l, reused across all m rows of B). The positions are KB consecutive slices k of H * IB
+// memory. A box holds P = 256 * W fibre positions x LB l (n_q l when n_q < LB), where
+// W = 16 bytes / element size is the number of consecutive positions one consumer thread owns
+// (one 128-bit shared-memory read per l, reused across all m rows of B). The positions are KB consecutive slices k of H * IB
 // consecutive i: with H = 1 the tensor map is (i, k, l) and IB a power of two covering inner
 // with little waste, so small inner extents still fill whole boxes; with H > 1 (few slices of
 // a large inner that IB divides) it is the 4D (i mod IB, i / IB, k, l). The dimensions are
@@ -510,7 +510,8 @@ struct StreamParams {
     int64_t tiles;          // ceil(outer / KB) * mper
     int64_t mper;           // ceil(inner / IB)
     int64_t units;          // tiles * S
-    int kchunks;            // ceil(nq / LB)
+    int kchunks;            // ceil(nq / lb)
+    int lb;                 // l per box: LB, or n_q when n_q < LB
     int kper;               // l chunks per unit
     int S;                  // l ranges per tile
     int b_cm;
@@ -542,8 +543,8 @@ __global__ void __maxnreg__(112)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int stages = P.stages;
     uint8_t* ring = smem;
-    T* bs = reinterpret_cast<T*>(smem + stages * kStreamBox);                  // [kper * LB][MB]
-    uint64_t* full = reinterpret_cast<uint64_t*>(bs + (size_t)P.kper * LB * MB);
+    T* bs = reinterpret_cast<T*>(smem + stages * kStreamBox);                  // [kper * lb][MB]
+    uint64_t* full = reinterpret_cast<uint64_t*>(bs + (size_t)P.kper * P.lb * MB);
     full = reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(full) + 15) & ~uintptr_t(15));
     uint64_t* empty = full + kStreamMaxStages;
     volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + kStreamMaxStages);
@@ -579,12 +580,12 @@ __global__ void __maxnreg__(112)
                 for (int kc = kc0; kc < kc1; ++kc) {
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&full[s], kStreamBox);
+                    mbar_expect_tx(&full[s], (uint32_t)(NP * P.lb * sizeof(T)));
                     if (P.h_shift == 0)
-                        tma_load_3d(ring + s * kStreamBox, &amap, &full[s], (int)(ib * IB), (int)(kb * P.kb), kc * LB);
+                        tma_load_3d(ring + s * kStreamBox, &amap, &full[s], (int)(ib * IB), (int)(kb * P.kb), kc * P.lb);
                     else
                         tma_load_4d(ring + s * kStreamBox, &amap, &full[s], 0, (int)(ib << P.h_shift), (int)(kb * P.kb),
-                                    kc * LB);
+                                    kc * P.lb);
                     if (++s == stages) { s = 0; ph ^= 1; }
                 }
             }
@@ -613,12 +614,12 @@ __global__ void __maxnreg__(112)
             const int64_t kb = t / mper, ib = t - kb * mper;
             const int kc0 = r * P.kper, kc1 = min(kc0 + P.kper, P.kchunks);
             if (r != staged) {
-                // stage rows [kc0 * LB, kc1 * LB) of B: bs[l][j] = B(j, l), zero outside B
+                // stage rows [kc0 * lb, kc1 * lb) of B: bs[l][j] = B(j, l), zero outside B
                 asm volatile("bar.sync 1, 256;" ::: "memory");
-                const int rows = (kc1 - kc0) * LB;
+                const int rows = (kc1 - kc0) * P.lb;
                 for (int e = tid; e < rows * MB; e += 256) {
                     const int lr = e / MB, j = e - lr * MB;
-                    const int64_t l = (int64_t)kc0 * LB + lr;
+                    const int64_t l = (int64_t)kc0 * P.lb + lr;
                     bs[e] = (j < P.m && l < P.nq) ? (P.b_cm ? Bg[j + l * P.m] : Bg[j * P.nq + l]) : T(0);
                 }
                 asm volatile("bar.sync 1, 256;" ::: "memory");
@@ -635,14 +636,16 @@ __global__ void __maxnreg__(112)
                 if (!have) ok = false;
                 if (have) {
                     const V* box = reinterpret_cast<const V*>(ring + s * kStreamBox) + tid;
-                    const T* brow = bs + (size_t)(kc - kc0) * LB * MB;
+                    const T* brow = bs + (size_t)(kc - kc0) * P.lb * MB;
+                    const int lb = P.lb;
                     // all LB reads up front, except at MB = 16 where the registers go to acc
                     constexpr int PRE = MB < 16 ? LB : 1;
                     V av[PRE];
 #pragma unroll
-                    for (int l = 0; l < PRE; ++l) av[l] = box[l * (NP / W)];
+                    for (int l = 0; l < PRE; ++l) av[l] = box[l * (NP / W)];   // in the stage even past lb
 #pragma unroll
                     for (int l = 0; l < LB; ++l) {
+                        if (l >= lb) break;
                         V a1;
                         if constexpr (PRE == 1) a1 = l == 0 ? av[0] : box[l * (NP / W)];
                         else a1 = av[l];
@@ -895,7 +898,8 @@ bool encode_stream_map(const View3& v, int dtype, int ib, int h, int kb, CUtenso
     EncodeTiledFn cuTensorMapEncodeTiled = encode_fn();
     if (!cuTensorMapEncodeTiled) return false;
     const size_t es = dtype == 0 ? 4 : 8;
-    const cuuint32_t lb = dtype == 0 ? (cuuint32_t)StreamGeom<float>::LB : (cuuint32_t)StreamGeom<double>::LB;
+    const cuuint32_t LB = dtype == 0 ? (cuuint32_t)StreamGeom<float>::LB : (cuuint32_t)StreamGeom<double>::LB;
+    const cuuint32_t lb = (cuuint64_t)v.nq < LB ? (cuuint32_t)v.nq : LB;
     const CUtensorMapDataType ty = dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     CUresult r;
     if (h <= 1) {
@@ -955,7 +959,7 @@ cudaError_t launch_stream_t(const CUtensorMap& amap, const StreamParams& P, size
 // Launch geometry of the TMA-fed small-m kernel (two CTAs per SM): box shape, ring depth, the
 // l split and the dynamic shared memory (ring + staged rows of B + barriers).
 struct StreamShape {
-    int ib, ib_shift, h_shift, kb, kchunks, kper, S, stages, mb;
+    int ib, ib_shift, h_shift, kb, lb, kchunks, kper, S, stages, mb;
     int64_t tiles, mper, units;
     size_t smem, ws_bytes;
 };
@@ -1003,9 +1007,10 @@ bool stream_shape(const View3& v, int dtype, int sms, StreamShape& sh)
     sh.mper = sh.h_shift ? ((v.inner >> sh.ib_shift) + (1 << sh.h_shift) - 1) >> sh.h_shift
                          : (v.inner + sh.ib - 1) / sh.ib;
     sh.tiles = ((v.outer + sh.kb - 1) / sh.kb) * sh.mper;
-    sh.kchunks = (int)((v.nq + LB - 1) / LB);
+    sh.lb = (int)std::min<int64_t>(LB, v.nq);
+    sh.kchunks = (int)((v.nq + sh.lb - 1) / sh.lb);
     const size_t budget = 112 * 1024 - 1024 - 256;   // per CTA, two per SM
-    const size_t row = (size_t)LB * sh.mb * es;      // staged B bytes per l chunk
+    const size_t row = (size_t)sh.lb * sh.mb * es;   // staged B bytes per l chunk
     int kper_max = 0;
     sh.stages = 0;
     for (int st = 6; st >= 4; --st)
@@ -1105,6 +1110,7 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
     P.mper = sh.mper;
     P.units = sh.units;
     P.kchunks = sh.kchunks;
+    P.lb = sh.lb;
     P.kper = sh.kper;
     P.S = sh.S;
     P.b_cm = v.b_cm;
