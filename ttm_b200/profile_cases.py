@@ -1,0 +1,72 @@
+"""One TTM case through the C ABI, repeated: the driver the committed ncu summaries are made with.
+
+    python -m ttm_b200.profile_cases --dtype f32 --precision bf16x3 --na 256,256,256,16 --q 2 \
+        --m 256 [--pia 1,2,3,4] [--iters 3]
+
+A (extents `na`, layout `pia`, dense) and B (m x n_q, column-major) are N(0,1) on the device,
+C is allocated on the device; the call is made `iters` times on the current stream. Prints the
+kernel the planner chose and the mean time per call (CUDA events, after one untimed call).
+"""
+from __future__ import annotations
+
+import argparse
+import math
+
+from . import _lib
+
+
+def _dense(n, pi):
+    w = [1] * len(n)
+    for r in range(1, len(n)):
+        w[pi[r] - 1] = w[pi[r - 1] - 1] * n[pi[r - 1] - 1]
+    return w
+
+
+def main():
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--precision", default="plain", choices=sorted(_lib.PRECISIONS))
+    ap.add_argument("--na", required=True, help="comma-separated extents")
+    ap.add_argument("--pia", default=None, help="comma-separated layout (default first-order)")
+    ap.add_argument("--q", type=int, required=True)
+    ap.add_argument("--m", type=int, required=True)
+    ap.add_argument("--iters", type=int, default=3)
+    a = ap.parse_args()
+    na = [int(x) for x in a.na.split(",")]
+    pia = [int(x) for x in a.pia.split(",")] if a.pia else list(range(1, len(na) + 1))
+    q, m = a.q, a.m
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    dt = _lib.F32 if a.dtype == "f32" else _lib.F64
+    tdt = torch.float32 if a.dtype == "f32" else torch.float64
+    n = math.prod(na)
+    nc = list(na)
+    nc[q - 1] = m
+    g = torch.Generator(device=dev).manual_seed(0)
+    A = torch.randn(n, device=dev, dtype=tdt, generator=g)
+    B = torch.randn(m * na[q - 1], device=dev, dtype=tdt, generator=g)
+    C = torch.empty(n // na[q - 1] * m, device=dev, dtype=tdt)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    prec = _lib.PRECISIONS[a.precision]
+
+    def run():
+        _lib.ttm_raw(dt, prec, q, len(na), A.data_ptr(), na, _dense(na, pia), pia, B.data_ptr(), [m, na[q - 1]],
+                     [1, 2], C.data_ptr(), nc, _dense(nc, pia), stream)
+
+    run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.iters):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / a.iters
+    es = 4 if a.dtype == "f32" else 8
+    gb = es * (n + n // na[q - 1] * m + m * na[q - 1]) / 1e9
+    print(f"kernel {_lib.last_kernel()}  {t:.3f} ms/call  {gb / (t / 1e3):.0f} GB/s algorithmic  "
+          f"{2.0 * m * n / (t / 1e3) / 1e12:.1f} TFLOP/s")
+
+
+if __name__ == "__main__":
+    main()
