@@ -147,7 +147,8 @@ enum tlibttm_schedule {
     TLIBTTM_SCHED_COLS_SPLIT = 3,  /* small-m kernel for strided fibres, l split over 8 warps (m <= 16, inner >= 2) */
     TLIBTTM_SCHED_ROWS = 4,        /* small-m kernel for contiguous fibres (m <= 16, q == pia[0]) */
     TLIBTTM_SCHED_TC_BF16X3 = 5,   /* tensor-core bf16x3, float only (FP32-accurate, not exact; m > 16) */
-    TLIBTTM_SCHED_COLS_TMA = 6,    /* small-m kernel for strided fibres fed by TMA (m <= 16, inner % 4 == 0) */
+    TLIBTTM_SCHED_COLS_TMA = 6,    /* small-m kernel fed by TMA (m <= 16): strided fibres (inner % 4 == 0), or
+                                      contiguous fibres of >= 16 floats / 8 doubles on 16-byte boundaries */
     TLIBTTM_SCHED_COUNT = 7
 };
 

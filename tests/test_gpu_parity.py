@@ -167,6 +167,41 @@ def test_stream_cols_box_shapes(cuda, oracle_c, dtype):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_stream_rows_contiguous_fibres(cuda, oracle_c, dtype):
+    """The TMA-fed small-m kernel in row mode (q = pi_1, contiguous fibres) through schedule 6:
+    partial l chunks, row counts off the 512-row tile (second box partly or wholly past the end), few tiles (l split with partial tiles added
+    by the last unit), a B restaged per unit, every m bucket; fibres that are too short or not
+    16-byte aligned are declined."""
+    import torch
+    from ttm_b200.selector import lib
+    rng = np.random.default_rng(41)
+    dt = _lib.F32 if dtype == np.float32 else _lib.F64
+    cases = [(20, 1000, 1), (256, 3000, 8), (64, 257, 16), (1000, 50, 3), (4096, 10, 2), (68, 70000, 4),
+             (3000, 7, 16), (16, 513, 5), (16, 100000, 8)]
+    if dtype == np.float64:
+        cases += [(18, 600, 5)]
+    declined = [(4, 1000, 1), (18, 100, 2)] if dtype == np.float32 else [(2, 1000, 1), (9, 100, 2)]
+    for n, (nq, outer, m) in enumerate(cases + declined):
+        na, pia, nc = [nq, outer], [1, 2], [m, outer]
+        md = dict(na=na, wa=ka.dense_strides(na, pia), pia=pia, nb=[m, nq], pib=[1, 2] if n % 2 else [2, 1],
+                  nc=nc, wc=ka.dense_strides(nc, pia))
+        a = rng.standard_normal(nq * outer).astype(dtype)
+        b = rng.standard_normal(m * nq).astype(dtype)
+        ta, tb = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+        tc = torch.full((m * outer,), float("nan"), dtype=ta.dtype, device=cuda)
+        rc = lib().tlibttm_ttm_sched(dt, 6, 1, 2, ta.data_ptr(), _lib.sz(na), _lib.sz(md["wa"]), _lib.sz(pia),
+                                     tb.data_ptr(), _lib.sz(md["nb"]), _lib.sz(md["pib"]), tc.data_ptr(), _lib.sz(nc),
+                                     _lib.sz(md["wc"]), None)
+        if (nq, outer, m) in declined:
+            assert rc == _lib.ERR_UNSUPPORTED, (nq, outer, m)
+            continue
+        assert rc == 0 and _lib.last_kernel() == "stream_rows", (nq, outer, m, rc)
+        ref = np.zeros(m * outer, dtype=dtype)
+        oracle_c.ttm(1, a, na, md["wa"], pia, b, md["nb"], md["pib"], ref, nc, md["wc"])
+        assert relerr(tc.cpu().numpy(), ref) <= (1e-14 if dtype == np.float64 else 2e-6), (nq, outer, m)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_short_contiguous_fibres(cuda, oracle_c, dtype):
     """q = pi_1 with n_q <= 16: rows of A are short and contiguous (the flat-tile row kernel);
     row counts that are not multiples of a warp's tile, n_q = 1, every m bucket, both B layouts."""
@@ -193,6 +228,7 @@ def test_kernel_selection_and_strided(cuda):
     cases = [([64, 32, 16], [1, 2, 3], 1, 4, "rowdot"),
              ([64, 32, 16], [1, 2, 3], 2, 8, "colvec"),
              ([256, 64, 512], [1, 2, 3], 2, 8, "stream_cols"),
+             ([256, 64, 512], [1, 2, 3], 1, 4, "stream_rows"),
              ([257, 64, 512], [1, 2, 3], 2, 8, "colvec"),
              ([64, 32, 16], [1, 2, 3], 2, 40, "simt_gemm"),
              ([64, 32, 16], [2, 3, 1], 2, 40, "simt_gemm")]

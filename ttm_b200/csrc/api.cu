@@ -37,6 +37,7 @@ const char* kernel_name(int id)
     case K_SPLIT_B: return "split_b";
     case K_GROUPED: return "grouped";
     case K_STREAM_COLS: return "stream_cols";
+    case K_STREAM_ROWS: return "stream_rows";
     default: return "";
     }
 }
@@ -211,12 +212,16 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
     v.b = x.b;
     v.c = x.c;
     if (v.m <= kSmallM) {
-        if (v.inner == 1) return note_launch(launch_rowdot(v, x.dtype, s), K_ROWDOT);
         // The TMA-fed kernel wins once A streams from HBM; below about half of L2 the plain
-        // column kernel's shorter start-up wins (both measured on L2-resident repeats).
+        // kernels' shorter start-up wins (both measured on L2-resident repeats). Contiguous
+        // fibres of at most 16 elements always take the flat-tile row kernel.
         const int64_t a_bytes = v.outer * v.nq * v.inner * (x.dtype == TLIBTTM_F32 ? 4 : 8);
-        if (a_bytes >= kStreamMinBytes && stream_supported(v, x.dtype))
-            return note_launch(launch_stream(v, x.dtype, s), K_STREAM_COLS);
+        const bool tma = a_bytes >= kStreamMinBytes && stream_supported(v, x.dtype);
+        if (v.inner == 1) {
+            if (tma && v.nq > 16) return note_launch(launch_stream(v, x.dtype, s), K_STREAM_ROWS);
+            return note_launch(launch_rowdot(v, x.dtype, s), K_ROWDOT);
+        }
+        if (tma) return note_launch(launch_stream(v, x.dtype, s), K_STREAM_COLS);
         return note_launch(launch_colvec(v, x.dtype, s), K_COLVEC);
     }
     if (precision == TLIBTTM_PREC_DEFAULT) precision = g_precision.load();
@@ -678,7 +683,8 @@ int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p, const voi
     case TLIBTTM_SCHED_COLS: return note_launch(launch_colvec_ls(v, dtype, 1, s), K_COLVEC);
     case TLIBTTM_SCHED_COLS_SPLIT: return note_launch(launch_colvec_ls(v, dtype, 8, s), K_COLVEC);
     case TLIBTTM_SCHED_ROWS: return note_launch(launch_rowdot(v, dtype, s), K_ROWDOT);
-    case TLIBTTM_SCHED_COLS_TMA: return note_launch(launch_stream(v, dtype, s), K_STREAM_COLS);
+    case TLIBTTM_SCHED_COLS_TMA:
+        return note_launch(launch_stream(v, dtype, s), v.inner == 1 ? K_STREAM_ROWS : K_STREAM_COLS);
     default: {
         int kid = K_NONE;
         e = launch_tc(v, TLIBTTM_PREC_BF16X3, s, &kid);

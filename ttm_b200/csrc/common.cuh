@@ -73,6 +73,7 @@ enum KernelId : int {
     K_SPLIT_B,
     K_GROUPED,
     K_STREAM_COLS,
+    K_STREAM_ROWS,
     K_COUNT
 };
 

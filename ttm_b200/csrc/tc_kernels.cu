@@ -30,6 +30,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <unordered_map>
 
 #include "tc_kernels.cuh"
@@ -525,25 +526,32 @@ template <typename T> struct V16Tc;
 template <> struct V16Tc<float> { using type = float4; };
 template <> struct V16Tc<double> { using type = double2; };
 
-template <typename T>
+// Column mode: W consecutive positions per thread, a 16 KB stage = one box of P positions x LB
+// l, [l][P]. Row mode (contiguous fibres, inner = 1): two fibres (rows) per thread, t and
+// t + 256; a 32 KB stage = two boxes of 256 rows x 64 bytes of l (LB = 16 float / 8 double),
+// each [row][64 bytes] with the 64-byte swizzle. Two rows per thread halve the shared-memory
+// reads of B per FMA; 64-byte rows keep the DRAM accesses long.
+template <typename T, bool ROWS = false>
 struct StreamGeom {
-    static constexpr int W = 16 / (int)sizeof(T);                      // positions per thread
-    static constexpr int P = 256 * W;                                  // positions per box
-    static constexpr int LB = (int)(kStreamBox / (P * sizeof(T)));     // l per box (4)
+    static constexpr int W = ROWS ? 2 : 16 / (int)sizeof(T);           // positions per thread
+    static constexpr int P = 256 * W;                                  // positions per stage
+    static constexpr uint32_t SB = ROWS ? 2 * kStreamBox : kStreamBox; // bytes per stage
+    static constexpr int LB = (int)(SB / (P * sizeof(T)));             // l per stage
 };
 
-template <typename T, int MB>
+template <typename T, int MB, bool ROWS>
 __global__ void __maxnreg__(112)
     stream_cols_kernel(const __grid_constant__ CUtensorMap amap, StreamParams P)
 {
-    using G = StreamGeom<T>;
+    using G = StreamGeom<T, ROWS>;
     constexpr int W = G::W, NP = G::P, LB = G::LB;
-    using V = typename V16Tc<T>::type;
+    using V = typename std::conditional<ROWS, T, typename V16Tc<T>::type>::type;   // W consecutive T
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int stages = P.stages;
     uint8_t* ring = smem;
-    T* bs = reinterpret_cast<T*>(smem + stages * kStreamBox);                  // [kper * lb][MB]
+    constexpr uint32_t SB = G::SB;
+    T* bs = reinterpret_cast<T*>(smem + stages * SB);                          // [kper * lb][MB]
     uint64_t* full = reinterpret_cast<uint64_t*>(bs + (size_t)P.kper * P.lb * MB);
     full = reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(full) + 15) & ~uintptr_t(15));
     uint64_t* empty = full + kStreamMaxStages;
@@ -581,10 +589,15 @@ __global__ void __maxnreg__(112)
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     issued[s] = (int)ph;
                     mbar_expect_tx(&full[s], (uint32_t)(NP * P.lb * sizeof(T)));
-                    if (P.h_shift == 0)
-                        tma_load_3d(ring + s * kStreamBox, &amap, &full[s], (int)(ib * IB), (int)(kb * P.kb), kc * P.lb);
+                    if (ROWS) {
+                        tma_load_2d(ring + s * SB, &amap, &full[s], kc * P.lb, (int)(kb * P.kb));
+                        tma_load_2d(ring + s * SB + SB / 2, &amap, &full[s], kc * P.lb,
+                                    (int)(kb * P.kb + 256));
+                    }
+                    else if (P.h_shift == 0)
+                        tma_load_3d(ring + s * SB, &amap, &full[s], (int)(ib * IB), (int)(kb * P.kb), kc * P.lb);
                     else
-                        tma_load_4d(ring + s * kStreamBox, &amap, &full[s], 0, (int)(ib << P.h_shift), (int)(kb * P.kb),
+                        tma_load_4d(ring + s * SB, &amap, &full[s], 0, (int)(ib << P.h_shift), (int)(kb * P.kb),
                                     kc * P.lb);
                     if (++s == stages) { s = 0; ph ^= 1; }
                 }
@@ -634,8 +647,53 @@ __global__ void __maxnreg__(112)
                 const bool got = ok && mbar_wait(&full[s], ph, abort_flag);
                 const bool have = __all_sync(0xffffffffu, got);
                 if (!have) ok = false;
-                if (have) {
-                    const V* box = reinterpret_cast<const V*>(ring + s * kStreamBox) + tid;
+                if (have && ROWS) {
+                    // rows tid and tid + 256: 64 bytes each, in four 16-byte chunks, chunk c stored
+                    // at c ^ ((row >> 1) & 3) (the 64-byte swizzle), which also keeps a warp's
+                    // reads free of bank conflicts; B is a broadcast read, used for both rows
+                    using V16 = typename V16Tc<T>::type;
+                    constexpr int EPC = 16 / (int)sizeof(T);
+                    const uint8_t* r0p = ring + s * SB + tid * 64;
+                    const uint8_t* r1p = r0p + SB / 2;
+                    const int sw = (tid >> 1) & 3;
+                    const T* brow = bs + (size_t)(kc - kc0) * LB * MB;
+                    V16 ch[2][4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        ch[0][c] = *reinterpret_cast<const V16*>(r0p + ((c ^ sw) << 4));
+                        ch[1][c] = *reinterpret_cast<const V16*>(r1p + ((c ^ sw) << 4));
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const T* a0 = reinterpret_cast<const T*>(&ch[0][c]);
+                        const T* a1 = reinterpret_cast<const T*>(&ch[1][c]);
+#pragma unroll
+                        for (int e = 0; e < EPC; ++e) {
+                            const T* bl = brow + (c * EPC + e) * MB;
+                            if constexpr (MB * sizeof(T) % 16 == 0) {
+#pragma unroll
+                                for (int q = 0; q < MB * (int)sizeof(T) / 16; ++q) {
+                                    const V16 bv = *reinterpret_cast<const V16*>(bl + q * EPC);
+                                    const T* b = reinterpret_cast<const T*>(&bv);
+#pragma unroll
+                                    for (int f = 0; f < EPC; ++f) {
+                                        acc[0][q * EPC + f] = fma(a0[e], b[f], acc[0][q * EPC + f]);
+                                        acc[1][q * EPC + f] = fma(a1[e], b[f], acc[1][q * EPC + f]);
+                                    }
+                                }
+                            } else {
+#pragma unroll
+                                for (int j = 0; j < MB; ++j) {
+                                    acc[0][j] = fma(a0[e], bl[j], acc[0][j]);
+                                    acc[1][j] = fma(a1[e], bl[j], acc[1][j]);
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s]);
+                } else if (have) {
+                    const V* box = reinterpret_cast<const V*>(ring + s * SB) + tid;
                     const T* brow = bs + (size_t)(kc - kc0) * P.lb * MB;
                     const int lb = P.lb;
                     // all LB reads up front, except at MB = 16 where the registers go to acc
@@ -674,6 +732,48 @@ __global__ void __maxnreg__(112)
                     if (lane == 0) mbar_arrive(&empty[s]);
                 }
                 if (++s == stages) { s = 0; ph ^= 1; }
+            }
+            if constexpr (ROWS) {
+                // rows k0 = tile * 512 + tid and k0 + 256; C[k][j] contiguous in j
+                const int64_t kr[2] = {kb * P.kb + tid, kb * P.kb + 256 + tid};
+                if (S == 1) {
+                    if (ok) {
+#pragma unroll
+                        for (int w = 0; w < 2; ++w)
+                            if (kr[w] < P.outer) {
+                                T* cp = C + kr[w] * P.m;
+#pragma unroll
+                                for (int j = 0; j < MB; ++j)
+                                    if (j < P.m) cp[j] = acc[w][j];
+                            }
+                    }
+                } else {
+                    T* wsp = static_cast<T*>(P.ws) + ((size_t)u * MB) * NP;
+#pragma unroll
+                    for (int j = 0; j < MB; ++j) {
+                        wsp[(size_t)j * NP + tid] = acc[0][j];
+                        wsp[(size_t)j * NP + 256 + tid] = acc[1][j];
+                    }
+                    __threadfence();
+                    asm volatile("bar.sync 1, 256;" ::: "memory");
+                    if (tid == 0) *last_flag = (!*abort_flag && atomicAdd(&P.cnt[t], 1u) == (unsigned)(S - 1)) ? 1 : 0;
+                    asm volatile("bar.sync 1, 256;" ::: "memory");
+                    if (*last_flag) {
+                        __threadfence();
+                        const T* w0 = static_cast<const T*>(P.ws) + ((size_t)t * S * MB) * NP;
+#pragma unroll
+                        for (int w = 0; w < 2; ++w) {
+                            if (kr[w] >= P.outer) continue;
+                            T* cp = C + kr[w] * P.m;
+                            for (int j = 0; j < MB && j < P.m; ++j) {
+                                T sum = T(0);
+                                for (int rr = 0; rr < S; ++rr) sum += __ldcg(w0 + ((size_t)rr * MB + j) * NP + w * 256 + tid);
+                                cp[j] = sum;
+                            }
+                        }
+                    }
+                }
+                continue;
             }
             const int64_t k = kb * P.kb + kk, i = (((ib << P.h_shift) + hh) << P.ib_shift) + ii;
             const bool mine = k < P.outer && i < P.inner;     // all W positions share k; inner % W == 0
@@ -934,41 +1034,87 @@ cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done)
     return e;
 }
 
-template <typename T, int MB>
+template <typename T, int MB, bool ROWS>
 cudaError_t launch_stream_mb(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
                              cudaStream_t s)
 {
     static std::atomic<uint64_t> done{0};
-    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB>, dev, done);
+    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS>, dev, done);
     if (e != cudaSuccess) return e;
-    stream_cols_kernel<T, MB><<<grid, kStreamThreads, smem, s>>>(amap, P);
+    stream_cols_kernel<T, MB, ROWS><<<grid, kStreamThreads, smem, s>>>(amap, P);
     return cudaGetLastError();
 }
 
-template <typename T>
+template <typename T, bool ROWS>
 cudaError_t launch_stream_t(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
                             cudaStream_t s)
 {
-    if (P.m <= 1) return launch_stream_mb<T, 1>(amap, P, smem, grid, dev, s);
-    if (P.m <= 2) return launch_stream_mb<T, 2>(amap, P, smem, grid, dev, s);
-    if (P.m <= 4) return launch_stream_mb<T, 4>(amap, P, smem, grid, dev, s);
-    if (P.m <= 8) return launch_stream_mb<T, 8>(amap, P, smem, grid, dev, s);
-    return launch_stream_mb<T, 16>(amap, P, smem, grid, dev, s);
+    if (P.m <= 1) return launch_stream_mb<T, 1, ROWS>(amap, P, smem, grid, dev, s);
+    if (P.m <= 2) return launch_stream_mb<T, 2, ROWS>(amap, P, smem, grid, dev, s);
+    if (P.m <= 4) return launch_stream_mb<T, 4, ROWS>(amap, P, smem, grid, dev, s);
+    if (P.m <= 8) return launch_stream_mb<T, 8, ROWS>(amap, P, smem, grid, dev, s);
+    return launch_stream_mb<T, 16, ROWS>(amap, P, smem, grid, dev, s);
+}
+
+// Row mode: A as the 2-D tensor map (l, row) of its contiguous fibres, boxes of LB l (64 bytes) x
+// 256 rows with the 64-byte swizzle.
+bool encode_rows_map(const View3& v, int dtype, CUtensorMap* map)
+{
+    EncodeTiledFn cuTensorMapEncodeTiled = encode_fn();
+    if (!cuTensorMapEncodeTiled) return false;
+    const size_t es = dtype == 0 ? 4 : 8;
+    cuuint64_t dims[2] = {(cuuint64_t)v.nq, (cuuint64_t)v.outer};
+    cuuint64_t strides[1] = {(cuuint64_t)v.nq * es};
+    cuuint32_t box[2] = {(cuuint32_t)(dtype == 0 ? StreamGeom<float, true>::LB : StreamGeom<double, true>::LB), 256};
+    cuuint32_t el[2] = {1, 1};
+    CUresult r = cuTensorMapEncodeTiled(map, dtype == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                                        2, const_cast<void*>(v.a), dims, strides, box, el,
+                                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
 }
 
 // Launch geometry of the TMA-fed small-m kernel (two CTAs per SM): box shape, ring depth, the
 // l split and the dynamic shared memory (ring + staged rows of B + barriers).
 struct StreamShape {
+    bool rows;
+    uint32_t sb;     // bytes per ring stage
     int ib, ib_shift, h_shift, kb, lb, kchunks, kper, S, stages, mb;
     int64_t tiles, mper, units;
     size_t smem, ws_bytes;
 };
 
+bool stream_tiles(const View3& v, size_t es, int W, int NP, StreamShape& sh);
+bool stream_split(const View3& v, size_t es, int NP, int LB, int sms, StreamShape& sh);
+
 bool stream_shape(const View3& v, int dtype, int sms, StreamShape& sh)
 {
     const size_t es = dtype == 0 ? 4 : 8;
-    const int W = 16 / (int)es, NP = 256 * W, LB = (int)(kStreamBox / (NP * es));
+    sh.rows = v.inner == 1;
+    // the kernel's geometry (StreamGeom) for this dtype and mode
+    const int W = es == 4 ? (sh.rows ? StreamGeom<float, true>::W : StreamGeom<float, false>::W)
+                          : (sh.rows ? StreamGeom<double, true>::W : StreamGeom<double, false>::W);
+    const uint32_t SB = sh.rows ? StreamGeom<float, true>::SB : StreamGeom<float, false>::SB;
+    sh.sb = SB;
+    const int NP = 256 * W, LB = (int)(SB / (NP * es));
     sh.mb = v.m <= 1 ? 1 : v.m <= 2 ? 2 : v.m <= 4 ? 4 : v.m <= 8 ? 8 : 16;
+    if (sh.rows) {
+        // one tile = 512 consecutive fibres; boxes always hold LB l (fibres of >= LB elements)
+        if (v.nq < LB) return false;
+        sh.ib_shift = sh.h_shift = 0;
+        sh.ib = 1;
+        sh.kb = 512;
+        sh.mper = 1;
+        sh.tiles = (v.outer + 511) / 512;
+    } else if (!stream_tiles(v, es, W, NP, sh)) {
+        return false;
+    }
+    return stream_split(v, es, NP, LB, sms, sh);
+}
+
+// Column mode: the box shape and tile count.
+bool stream_tiles(const View3& v, size_t es, int W, int NP, StreamShape& sh)
+{
     // Box shape: among the shapes whose boxes are at most 20% out-of-range fill (positions past
     // inner or outer), the one with the fewest positions, where rows under 32 bytes count
     // double (they use half of each DRAM sector they touch). Candidates: (IB, H = 1) with IB a
@@ -1007,21 +1153,29 @@ bool stream_shape(const View3& v, int dtype, int sms, StreamShape& sh)
     sh.mper = sh.h_shift ? ((v.inner >> sh.ib_shift) + (1 << sh.h_shift) - 1) >> sh.h_shift
                          : (v.inner + sh.ib - 1) / sh.ib;
     sh.tiles = ((v.outer + sh.kb - 1) / sh.kb) * sh.mper;
+    return true;
+}
+
+// Both modes: ring depth, the l split and the shared memory.
+bool stream_split(const View3& v, size_t es, int NP, int LB, int sms, StreamShape& sh)
+{
     sh.lb = (int)std::min<int64_t>(LB, v.nq);
     sh.kchunks = (int)((v.nq + sh.lb - 1) / sh.lb);
     const size_t budget = 112 * 1024 - 1024 - 256;   // per CTA, two per SM
     const size_t row = (size_t)sh.lb * sh.mb * es;   // staged B bytes per l chunk
+    // ring of 96 KB when B fits beside it, down to 64 KB; otherwise 80 KB (64 KB for 32 KB stages)
+    // and B staged a part at a time
     int kper_max = 0;
     sh.stages = 0;
-    for (int st = 6; st >= 4; --st)
-        if ((size_t)sh.kchunks * row <= budget - (size_t)st * kStreamBox) {
+    for (int st = (int)(96 * 1024 / sh.sb); st >= (int)(64 * 1024 / sh.sb); --st)
+        if ((size_t)st * sh.sb + (size_t)sh.kchunks * row <= budget) {
             sh.stages = st;
             kper_max = sh.kchunks;
             break;
         }
     if (!sh.stages) {
-        sh.stages = 5;
-        kper_max = (int)((budget - 5 * (size_t)kStreamBox) / row);
+        sh.stages = (int)(80 * 1024 / sh.sb);
+        kper_max = (int)((budget - (size_t)sh.stages * sh.sb) / row);
     }
     // l split: the S (at least enough for B to fit) with the shortest estimated makespan, in
     // boxes: rounds of units over the CTA slots x (boxes per unit + 1 for the pipeline ramp
@@ -1042,7 +1196,7 @@ bool stream_shape(const View3& v, int dtype, int sms, StreamShape& sh)
     }
     sh.S = (sh.kchunks + sh.kper - 1) / sh.kper;
     sh.units = sh.tiles * sh.S;
-    sh.smem = 1024 + (size_t)sh.stages * kStreamBox + (size_t)sh.kper * row + 256;
+    sh.smem = 1024 + (size_t)sh.stages * sh.sb + (size_t)sh.kper * row + 256;
     sh.ws_bytes = sh.S > 1 ? (size_t)sh.units * sh.mb * NP * es : 0;
     return true;
 }
@@ -1072,11 +1226,17 @@ bool permuted_maps_ok()
 
 bool stream_supported(const View3& v, int dtype)
 {
-    if (!permuted_maps_ok()) return false;
-    // 16-byte rows and 16-byte vectors of W consecutive positions in A and C
     const int64_t w = dtype == 0 ? 4 : 2;
-    if (v.m > kSmallM || v.inner < w || v.inner % w != 0) return false;
-    if (((reinterpret_cast<uintptr_t>(v.a) | reinterpret_cast<uintptr_t>(v.c)) & 15u) != 0) return false;
+    if (v.m > kSmallM) return false;
+    if (v.inner == 1) {
+        // row mode: fibres start on 16-byte boundaries (the tensor map's row stride)
+        if (v.nq % w != 0 || (reinterpret_cast<uintptr_t>(v.a) & 15u) != 0) return false;
+    } else {
+        if (!permuted_maps_ok()) return false;
+        // 16-byte rows and 16-byte vectors of W consecutive positions in A and C
+        if (v.inner < w || v.inner % w != 0) return false;
+        if (((reinterpret_cast<uintptr_t>(v.a) | reinterpret_cast<uintptr_t>(v.c)) & 15u) != 0) return false;
+    }
     if (v.outer >= (int64_t(1) << 31) || v.nq >= (int64_t(1) << 31) || v.inner >= (int64_t(1) << 31)) return false;
     // shapes whose boxes would be mostly out-of-range fill go elsewhere
     StreamShape sh;
@@ -1097,7 +1257,8 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
     StreamShape sh;
     if (!stream_shape(v, dtype, g_sm_count, sh)) return cudaErrorNotSupported;
     CUtensorMap amap;
-    if (!encode_stream_map(v, dtype, sh.ib, 1 << sh.h_shift, sh.kb, &amap)) return cudaErrorInvalidValue;
+    if (sh.rows ? !encode_rows_map(v, dtype, &amap) : !encode_stream_map(v, dtype, sh.ib, 1 << sh.h_shift, sh.kb, &amap))
+        return cudaErrorInvalidValue;
     StreamParams P{};
     P.b = v.b;
     P.c = v.c;
@@ -1128,8 +1289,10 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
     }
     const int grid = (int)std::min<int64_t>(sh.units, (int64_t)g_sm_count * 2);
     if (e == cudaSuccess)
-        e = dtype == 0 ? launch_stream_t<float>(amap, P, sh.smem, grid, dev, s)
-                       : launch_stream_t<double>(amap, P, sh.smem, grid, dev, s);
+        e = sh.rows ? (dtype == 0 ? launch_stream_t<float, true>(amap, P, sh.smem, grid, dev, s)
+                                  : launch_stream_t<double, true>(amap, P, sh.smem, grid, dev, s))
+                    : (dtype == 0 ? launch_stream_t<float, false>(amap, P, sh.smem, grid, dev, s)
+                                  : launch_stream_t<double, false>(amap, P, sh.smem, grid, dev, s));
     if (scratch) cudaFreeAsync(scratch, s);
     return e;
 }

@@ -351,7 +351,8 @@ def _heuristic_in(pr, allowed):
     inner, nq, outer = geometry(pr["na"], pr["pia"], pr["q"])
     if pr["m"] <= 16:
         if inner == 1:
-            return 4
+            big = math.prod(pr["na"]) * 4 >= 64 << 20
+            return 6 if (6 in allowed and big and nq > 16 and valid_mask(pr)[5]) else 4
         if 6 in allowed and math.prod(pr["na"]) * 4 >= 64 << 20 and valid_mask(pr)[5]:
             return 6
         rv = 4
