@@ -59,6 +59,11 @@ CASES = [
     ([96, 33, 300], [1, 2, 3], 1, 64, True),      # q = pi_1: K-major tiles, partial K chunk (96 = 3 x 32)
     ([132, 20, 70], [1, 3, 2], 1, 48, False),     # q = pi_1, partial M tile (outer 1400), nq 132
     ([40, 30, 20, 12], [2, 4, 1, 3], 1, 32, True),  # inner 30*12=360 under a permuted layout
+    # rows not 16-byte aligned for TMA: the converter warps load A themselves
+    ([33, 40, 7], [1, 2, 3], 2, 64, True),        # inner 33 (odd), partial M tile
+    ([135, 19, 11], [1, 2, 3], 2, 40, False),     # inner 135, nq 19, partial K chunk
+    ([37, 20, 30], [1, 2, 3], 1, 48, True),       # q = pi_1 with nq 37 (K-major tiles)
+    ([21, 17, 300], [1, 3, 2], 1, 20, False),     # q = pi_1, nq 21, outer 5100
 ]
 
 

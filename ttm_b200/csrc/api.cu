@@ -519,6 +519,13 @@ int run(const Args& x, int precision, void* stream)
 // Under precision auto, a batched problem takes the tensor-core path only from this many
 // elements of A on; smaller ones run inside the grouped launch.
 constexpr int64_t kAutoTcMinElems = int64_t(1) << 22;
+// Batched plans: problems with at least this many elements of A take their own launch of the
+// kernel the planner picks for them (bf16x3 under auto/bf16x3 for m > 16, the small-m kernels
+// for m <= 16); smaller ones share the grouped launch. Measured on the 512-problem workload, the
+// specialised kernels beat the grouped launch's generic tiles well below the single-call
+// threshold above.
+constexpr int64_t kPlanSingleMinElems = int64_t(1) << 18;
+constexpr int kPlanStreams = 4;     // worker streams the singles of a batched plan spread over
 
 struct Single {            // one problem launched on its own inside a plan
     int dtype;
@@ -568,6 +575,10 @@ struct tlibttm_plan_s {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t own = nullptr;
+    // fork/join of batched singles: worker streams and their events (created on first run)
+    cudaStream_t workers[tlibttm::kPlanStreams] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t joins[tlibttm::kPlanStreams] = {};
 };
 
 namespace tlibttm {
@@ -576,15 +587,38 @@ namespace {
 int plan_run_impl(tlibttm_plan* P, cudaStream_t s)
 {
     int rc;
+    cudaError_t e;
+    // Batched plans with several singles fork them over worker streams (largest first, round
+    // robin) and join them back into s; chain plans run their steps in order on s.
+    const bool fan = P->type == 0 && P->singles.size() > 1;
+    if (fan) {
+        if (!P->fork) {
+            if ((e = cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "cudaEventCreate");
+            for (int w = 0; w < kPlanStreams; ++w)
+                if ((e = cudaStreamCreateWithFlags(&P->workers[w], cudaStreamNonBlocking)) != cudaSuccess ||
+                    (e = cudaEventCreateWithFlags(&P->joins[w], cudaEventDisableTiming)) != cudaSuccess)
+                    return cuda_fail(e, "cudaStreamCreate");
+        }
+        if ((e = cudaEventRecord(P->fork, s)) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        for (int w = 0; w < kPlanStreams; ++w)
+            if ((e = cudaStreamWaitEvent(P->workers[w], P->fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+    }
     if (P->type == 0 && P->total > 0) {
-        cudaError_t e = cudaMemsetAsync(P->d_queue, 0, sizeof(unsigned long long), s);
+        e = cudaMemsetAsync(P->d_queue, 0, sizeof(unsigned long long), s);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
         if ((rc = note_launch(launch_grouped(P->d_desc, (int)P->descs.size(), P->total, P->d_queue, P->dtype, P->grid, s),
                               K_GROUPED)))
             return rc;
     }
-    for (Single& sg : P->singles)
-        if ((rc = run_single(sg, P->precision, s))) return rc;
+    for (size_t i = 0; i < P->singles.size(); ++i)
+        if ((rc = run_single(P->singles[i], P->precision, fan ? P->workers[i % kPlanStreams] : s))) return rc;
+    if (fan) {
+        for (int w = 0; w < kPlanStreams; ++w) {
+            if ((e = cudaEventRecord(P->joins[w], P->workers[w])) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+            if ((e = cudaStreamWaitEvent(s, P->joins[w], 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+        }
+    }
     return TLIBTTM_OK;
 }
 
@@ -598,6 +632,11 @@ void plan_free(tlibttm_plan* P)
     for (void* b : P->bufs)
         if (b) cudaFree(b);
     if (P->own) cudaStreamDestroy(P->own);
+    for (int w = 0; w < kPlanStreams; ++w) {
+        if (P->workers[w]) cudaStreamDestroy(P->workers[w]);
+        if (P->joins[w]) cudaEventDestroy(P->joins[w]);
+    }
+    if (P->fork) cudaEventDestroy(P->fork);
     delete P;
 }
 
@@ -741,7 +780,7 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
     v.c = x.c;
     if (!tc_supported(v, TLIBTTM_PREC_BF16X3))
         return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm_ttm_f32_bf16x3_noalloc: shape not handled by the tensor-core "
-                                             "kernel (needs m > 16, and inner % 4 == 0 or q = pi_1 with n_q % 4 == 0).");
+                                             "kernel (needs m > 16, and inner >= 32 or q = pi_1).");
     if (tc_image_bytes(v) > kNoAllocImageBytes)
         return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_f32_bf16x3_noalloc: B needs a " + std::to_string(tc_image_bytes(v)) +
                                          "-byte split image; this entry point holds at most " +
@@ -792,15 +831,18 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                     v.a = x.a;
                     v.b = x.b;
                     v.c = x.c;
-                    bool tc = false;
+                    bool single = false;
+                    const int64_t elems = v.outer * v.inner * v.nq;
                     if (pl.dense && v.m > kSmallM && dtype == TLIBTTM_F32) {
-                        // bf16x3 is asked for explicitly: every supported problem takes it. Under auto,
-                        // only large problems do; small ones are cheaper inside the grouped launch.
-                        if (prec == TLIBTTM_PREC_BF16X3) tc = tc_supported(v, TLIBTTM_PREC_BF16X3);
+                        // bf16x3 asked for explicitly: every supported problem takes it; under auto,
+                        // supported problems above the single-launch size
+                        if (prec == TLIBTTM_PREC_BF16X3) single = tc_supported(v, TLIBTTM_PREC_BF16X3);
                         if (prec == TLIBTTM_PREC_AUTO)
-                            tc = tc_supported(v, TLIBTTM_PREC_BF16X3) && v.outer * v.inner * v.nq >= kAutoTcMinElems;
+                            single = tc_supported(v, TLIBTTM_PREC_BF16X3) && elems >= kPlanSingleMinElems;
                     }
-                    if (!pl.dense || tc) {
+                    // small m: the small-m kernels (column, row, TMA-fed) above the single-launch size
+                    if (pl.dense && v.m <= kSmallM && elems >= kPlanSingleMinElems) single = true;
+                    if (!pl.dense || single) {
                         P->singles.push_back(Single{dtype, x.a, x.b, x.c, pl});
                     } else {
                         GroupDesc d{};
@@ -850,6 +892,13 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
         if (rc) return fail(rc, problem_prefix(i) + g_err);
     }
     std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) { return x.cost > y.cost; });
+    // singles largest first, so that the round robin over the worker streams balances them
+    auto work = [](const Single& sg) {
+        const View3& v = sg.pl.v;
+        return (double)v.outer * v.inner * v.nq * (1.0 + (double)v.m / 16.0);
+    };
+    std::stable_sort(P->singles.begin(), P->singles.end(),
+                     [&](const Single& x, const Single& y) { return work(x) > work(y); });
     int64_t first = 0;
     for (Item& it : items) {
         it.d.first = first;

@@ -89,6 +89,8 @@ __device__ __forceinline__ uint32_t mnmaj_sw128_off(uint32_t l, uint32_t ichunk)
 
 struct TcParams {
     float* c;
+    const float* a;          // A itself, for the converters' own loads (ldg_a)
+    int ldg_a;               // A rows not 16-byte aligned for TMA: the converters load A
     const uint8_t* bimg;     // pre-split B: [jb][kc][hi|lo][NT rows x 32 B]
     int* status;             // device status word (0 = ok)
     int64_t outer, nq, inner, m;
@@ -218,6 +220,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int64_t mt = t % P.tiles_m;
                 for (int kc = 0; kc < kchunks; ++kc) {
                     if (!mbar_wait(&a_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    if (P.ldg_a) {
+                        // no copy: the stage is free for the converters, which load A themselves
+                        mbar_arrive(&a_full[s]);
+                        if (++s == AS) { s = 0; ph ^= 1; }
+                        continue;
+                    }
                     issued[s] = (int)ph;
                     mbar_expect_tx(&a_full[s], L.a_bytes);
                     if (GEOM == GEOM_MN) {
@@ -332,16 +340,42 @@ __global__ void __launch_bounds__(kThreads, 1)
                 uint8_t* buf = a_at(s);
                 float4 x[kIters];
                 uint32_t off[kIters];
+                // tile origin for the converters' own loads of A (ldg_a): slice k / first row
+                const int64_t mt = t % P.tiles_m;
+                const int64_t tk = GEOM == GEOM_MN ? mt / mper : 0;
+                const int64_t r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
 #pragma unroll
                 for (int it = 0; it < kIters; ++it) {
                     const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
                     if (GEOM == GEOM_MN) {
                         const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
-                        if (have) x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
+                        if (have && P.ldg_a) {
+                            // elements (l, i .. i+3) of slice tk, zero outside A
+                            const int64_t gl = (int64_t)kc * kBK + l, i = r0 + w * 4;
+                            const float* src = P.a + (tk * P.nq + gl) * P.inner + i;
+                            const bool lv = gl < P.nq;
+                            x[it].x = (lv && i < P.inner) ? __ldg(src) : 0.0f;
+                            x[it].y = (lv && i + 1 < P.inner) ? __ldg(src + 1) : 0.0f;
+                            x[it].z = (lv && i + 2 < P.inner) ? __ldg(src + 2) : 0.0f;
+                            x[it].w = (lv && i + 3 < P.inner) ? __ldg(src + 3) : 0.0f;
+                        } else if (have) {
+                            x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
+                        }
                         off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
                     } else {
                         const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
-                        if (have) x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                        if (have && P.ldg_a) {
+                            // elements (row, l .. l+3) of the contiguous fibre row, zero outside A
+                            const int64_t row = r0 + k, gl = (int64_t)kc * kBK + lc * 4;
+                            const float* src = P.a + row * P.nq + gl;
+                            const bool rv = row < P.outer;
+                            x[it].x = (rv && gl < P.nq) ? __ldg(src) : 0.0f;
+                            x[it].y = (rv && gl + 1 < P.nq) ? __ldg(src + 1) : 0.0f;
+                            x[it].z = (rv && gl + 2 < P.nq) ? __ldg(src + 2) : 0.0f;
+                            x[it].w = (rv && gl + 3 < P.nq) ? __ldg(src + 3) : 0.0f;
+                        } else if (have) {
+                            x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                        }
                         off[it] = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
                     }
                 }
@@ -539,8 +573,12 @@ struct StreamGeom {
     static constexpr int LB = (int)(SB / (P * sizeof(T)));             // l per stage
 };
 
-template <typename T, int MB, bool ROWS>
-__global__ void __maxnreg__(112)
+// The kernel comes in two builds: 112 registers per thread (two CTAs of 288 threads per SM) and
+// a lean 72 (three CTAs per SM), which fits without spills for m <= 4, and m <= 8 in float.
+constexpr bool stream_lean_ok(int mb, size_t es) { return mb <= 4 || (mb <= 8 && es == 4); }
+
+template <typename T, int MB, bool ROWS, bool LEAN>
+__global__ void __maxnreg__(LEAN ? 72 : 112)
     stream_cols_kernel(const __grid_constant__ CUtensorMap amap, StreamParams P)
 {
     using G = StreamGeom<T, ROWS>;
@@ -941,10 +979,14 @@ bool encode_c_map(const View3& v, int geom, CUtensorMap* map)
     return r == CUDA_SUCCESS;
 }
 
-int geometry_of(const View3& v)
+int geometry_of(const View3& v) { return v.inner == 1 ? GEOM_K : GEOM_MN; }
+
+// A's rows (the fibres' 16-l chunks for GEOM_K, the i runs for GEOM_MN) start on 16-byte
+// boundaries: TMA can load its tiles. Otherwise the converter warps load A themselves.
+bool tma_a_ok(const View3& v, int geom)
 {
-    if (v.inner == 1) return (v.nq % 4 == 0) ? GEOM_K : -1;
-    return (v.inner % 4 == 0) ? GEOM_MN : -1;
+    if ((reinterpret_cast<uintptr_t>(v.a) & 15u) != 0) return false;
+    return geom == GEOM_K ? v.nq % 4 == 0 : v.inner % 4 == 0;
 }
 
 // Splits B into `img` (tc_image_bytes(v) bytes) and launches the bf16x3 kernel for v on stream s.
@@ -955,8 +997,11 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     const int jblocks = (int)((v.m + nt - 1) / nt);
     const int kchunks = (int)((v.nq + kBK - 1) / kBK);
     CUtensorMap amap, cmap;
-    if (!encode_a_map(v, geom, &amap)) return cudaErrorInvalidValue;
     TcParams P{};
+    P.ldg_a = tma_a_ok(v, geom) ? 0 : 1;
+    P.a = static_cast<const float*>(v.a);
+    if (P.ldg_a) std::memset(&amap, 0, sizeof(amap));
+    else if (!encode_a_map(v, geom, &amap)) return cudaErrorInvalidValue;
     P.tma_c = encode_c_map(v, geom, &cmap) ? 1 : 0;
     if (!P.tma_c) std::memset(&cmap, 0, sizeof(cmap));
     P.c = static_cast<float*>(v.c);
@@ -1023,37 +1068,51 @@ bool encode_stream_map(const View3& v, int dtype, int ib, int h, int kb, CUtenso
     return r == CUDA_SUCCESS;
 }
 
-// cudaFuncSetAttribute once per kernel instance and device (devices 0..63).
+// cudaFuncSetAttribute once per kernel instance and device (devices 0..63): the full dynamic
+// shared memory, and for instances meant to run three CTAs per SM the largest shared-memory
+// carveout (three CTAs of ~74 KB).
 template <typename K>
-cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done)
+cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done, bool max_carveout = false)
 {
     const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
     if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess && max_carveout)
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
     return e;
 }
 
-template <typename T, int MB, bool ROWS>
+template <typename T, int MB, bool ROWS, bool LEAN>
 cudaError_t launch_stream_mb(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
                              cudaStream_t s)
 {
     static std::atomic<uint64_t> done{0};
-    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS>, dev, done);
+    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS, LEAN>, dev, done, LEAN);
     if (e != cudaSuccess) return e;
-    stream_cols_kernel<T, MB, ROWS><<<grid, kStreamThreads, smem, s>>>(amap, P);
+    stream_cols_kernel<T, MB, ROWS, LEAN><<<grid, kStreamThreads, smem, s>>>(amap, P);
     return cudaGetLastError();
+}
+
+template <typename T, int MB, bool ROWS>
+cudaError_t launch_stream_lean(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
+                               bool lean, cudaStream_t s)
+{
+    if constexpr (MB <= 4 || (MB <= 8 && sizeof(T) == 4)) {
+        if (lean) return launch_stream_mb<T, MB, ROWS, true>(amap, P, smem, grid, dev, s);
+    }
+    return launch_stream_mb<T, MB, ROWS, false>(amap, P, smem, grid, dev, s);
 }
 
 template <typename T, bool ROWS>
 cudaError_t launch_stream_t(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
-                            cudaStream_t s)
+                            bool lean, cudaStream_t s)
 {
-    if (P.m <= 1) return launch_stream_mb<T, 1, ROWS>(amap, P, smem, grid, dev, s);
-    if (P.m <= 2) return launch_stream_mb<T, 2, ROWS>(amap, P, smem, grid, dev, s);
-    if (P.m <= 4) return launch_stream_mb<T, 4, ROWS>(amap, P, smem, grid, dev, s);
-    if (P.m <= 8) return launch_stream_mb<T, 8, ROWS>(amap, P, smem, grid, dev, s);
-    return launch_stream_mb<T, 16, ROWS>(amap, P, smem, grid, dev, s);
+    if (P.m <= 1) return launch_stream_lean<T, 1, ROWS>(amap, P, smem, grid, dev, lean, s);
+    if (P.m <= 2) return launch_stream_lean<T, 2, ROWS>(amap, P, smem, grid, dev, lean, s);
+    if (P.m <= 4) return launch_stream_lean<T, 4, ROWS>(amap, P, smem, grid, dev, lean, s);
+    if (P.m <= 8) return launch_stream_lean<T, 8, ROWS>(amap, P, smem, grid, dev, lean, s);
+    return launch_stream_lean<T, 16, ROWS>(amap, P, smem, grid, dev, lean, s);
 }
 
 // Row mode: A as the 2-D tensor map (l, row) of its contiguous fibres, boxes of LB l (64 bytes) x
@@ -1079,7 +1138,7 @@ bool encode_rows_map(const View3& v, int dtype, CUtensorMap* map)
 struct StreamShape {
     bool rows;
     uint32_t sb;     // bytes per ring stage
-    int ib, ib_shift, h_shift, kb, lb, kchunks, kper, S, stages, mb;
+    int ib, ib_shift, h_shift, kb, lb, kchunks, kper, S, stages, mb, per_sm;
     int64_t tiles, mper, units;
     size_t smem, ws_bytes;
 };
@@ -1161,27 +1220,35 @@ bool stream_split(const View3& v, size_t es, int NP, int LB, int sms, StreamShap
 {
     sh.lb = (int)std::min<int64_t>(LB, v.nq);
     sh.kchunks = (int)((v.nq + sh.lb - 1) / sh.lb);
-    const size_t budget = 112 * 1024 - 1024 - 256;   // per CTA, two per SM
+    // per CTA: two or three CTAs per SM share its 228 KB of shared memory (1 KB each reserved).
+    // Three (the lean build, m = 3..8) only when the tiles alone leave CTA slots of two per SM
+    // empty: measured, the smaller ring and B stage of three CTAs cost more than the extra warps
+    // gain when there are tiles enough, or when m <= 2 keeps the consumers light.
+    sh.per_sm = (stream_lean_ok(sh.mb, es) && sh.mb >= 4 && sh.tiles < 2 * (int64_t)sms) ? 3 : 2;
+    const size_t budget = (sh.per_sm == 3 ? 74 : 112) * 1024 - 1024 - 256;
     const size_t row = (size_t)sh.lb * sh.mb * es;   // staged B bytes per l chunk
-    // ring of 96 KB when B fits beside it, down to 64 KB; otherwise 80 KB (64 KB for 32 KB stages)
-    // and B staged a part at a time
+    // ring per CTA (192 KB in flight per SM either way): two CTAs 96 KB when B fits beside it,
+    // down to 64 KB, otherwise 80 KB; three CTAs 64 KB down to 48 KB, otherwise 48 KB; B staged
+    // a part at a time when it does not fit; at least two stages
+    const size_t hi = sh.per_sm == 3 ? 64 * 1024 : 96 * 1024, lo = sh.per_sm == 3 ? 48 * 1024 : 64 * 1024,
+                 fb = sh.per_sm == 3 ? 48 * 1024 : 80 * 1024;
     int kper_max = 0;
     sh.stages = 0;
-    for (int st = (int)(96 * 1024 / sh.sb); st >= (int)(64 * 1024 / sh.sb); --st)
+    for (int st = std::max<int>(2, (int)(hi / sh.sb)); st >= std::max<int>(2, (int)(lo / sh.sb)); --st)
         if ((size_t)st * sh.sb + (size_t)sh.kchunks * row <= budget) {
             sh.stages = st;
             kper_max = sh.kchunks;
             break;
         }
     if (!sh.stages) {
-        sh.stages = (int)(80 * 1024 / sh.sb);
+        sh.stages = std::max<int>(2, (int)(fb / sh.sb));
         kper_max = (int)((budget - (size_t)sh.stages * sh.sb) / row);
     }
     // l split: the S (at least enough for B to fit) with the shortest estimated makespan, in
     // boxes: rounds of units over the CTA slots x (boxes per unit + 1 for the pipeline ramp
     // + 3 + MB / 2 for writing, fencing and re-reading a partial tile when S > 1); a split must
     // win by 10% (measured: splits cost more than this model says)
-    const int64_t slots = 2 * (int64_t)sms;
+    const int64_t slots = (int64_t)sh.per_sm * sms;
     const int64_t s_min = (sh.kchunks + kper_max - 1) / kper_max;
     const int64_t s_max = std::max<int64_t>(s_min, std::min<int64_t>(sh.kchunks, 64));
     double best_t = 0;
@@ -1287,12 +1354,14 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
         P.cnt = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(scratch) + ws);
         e = cudaMemsetAsync(P.cnt, 0, (size_t)sh.tiles * sizeof(unsigned), s);
     }
-    const int grid = (int)std::min<int64_t>(sh.units, (int64_t)g_sm_count * 2);
-    if (e == cudaSuccess)
-        e = sh.rows ? (dtype == 0 ? launch_stream_t<float, true>(amap, P, sh.smem, grid, dev, s)
-                                  : launch_stream_t<double, true>(amap, P, sh.smem, grid, dev, s))
-                    : (dtype == 0 ? launch_stream_t<float, false>(amap, P, sh.smem, grid, dev, s)
-                                  : launch_stream_t<double, false>(amap, P, sh.smem, grid, dev, s));
+    const int grid = (int)std::min<int64_t>(sh.units, (int64_t)g_sm_count * sh.per_sm);
+    if (e == cudaSuccess) {
+        const bool lean = sh.per_sm == 3;
+        e = sh.rows ? (dtype == 0 ? launch_stream_t<float, true>(amap, P, sh.smem, grid, dev, lean, s)
+                                  : launch_stream_t<double, true>(amap, P, sh.smem, grid, dev, lean, s))
+                    : (dtype == 0 ? launch_stream_t<float, false>(amap, P, sh.smem, grid, dev, lean, s)
+                                  : launch_stream_t<double, false>(amap, P, sh.smem, grid, dev, lean, s));
+    }
     if (scratch) cudaFreeAsync(scratch, s);
     return e;
 }
@@ -1310,8 +1379,7 @@ bool tc_supported(const View3& v, int precision)
     if (precision != TLIBTTM_PREC_BF16X3) return false;
     if (v.m <= kSmallM) return false;
     const int g = geometry_of(v);
-    if (g < 0) return false;
-    if ((reinterpret_cast<uintptr_t>(v.a) & 15u) != 0) return false;
+    if ((reinterpret_cast<uintptr_t>(v.a) & 3u) != 0) return false;   // float-aligned A
     if (g == GEOM_MN && v.inner < 32) return false;
     // TMA coordinates are signed 32-bit.
     if (v.outer >= (int64_t(1) << 31) || v.nq >= (int64_t(1) << 31) || v.inner >= (int64_t(1) << 31)) return false;
