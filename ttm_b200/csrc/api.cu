@@ -197,9 +197,10 @@ int note_launch(cudaError_t e, int kid)
 }
 
 constexpr int64_t kStreamMinBytes = int64_t(64) << 20;
+constexpr int64_t kPlanStreamMinBytes = int64_t(4) << 20;
 
 // All operands are device memory: enqueue on stream s.
-int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
+int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s, int64_t stream_min_bytes = kStreamMinBytes)
 {
     if (!pl.dense) {
         pl.sp.a = x.a;
@@ -216,7 +217,7 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s)
         // kernels' shorter start-up wins (both measured on L2-resident repeats). Contiguous
         // fibres of at most 16 elements always take the flat-tile row kernel.
         const int64_t a_bytes = v.outer * v.nq * v.inner * (x.dtype == TLIBTTM_F32 ? 4 : 8);
-        const bool tma = a_bytes >= kStreamMinBytes && stream_supported(v, x.dtype);
+        const bool tma = a_bytes >= stream_min_bytes && stream_supported(v, x.dtype);
         if (v.inner == 1) {
             if (tma && v.nq > 16) return note_launch(launch_stream(v, x.dtype, s), K_STREAM_ROWS);
             return note_launch(launch_rowdot(v, x.dtype, s), K_ROWDOT);
@@ -542,7 +543,8 @@ int run_single(Single& sg, int precision, cudaStream_t s)
     x.a = sg.a;
     x.b = sg.b;
     x.c = sg.c;
-    return run_device(x, sg.pl, precision, s);
+    // a plan streams many problems through HBM: the TMA-fed small-m kernel pays off from 4 MB
+    return run_device(x, sg.pl, precision, s, kPlanStreamMinBytes);
 }
 
 // Kernels run_device launches for a plan entry (tensor-core paths launch two).
