@@ -238,7 +238,8 @@ def run_extra_workloads(dev, stream):
     by = sum(workloads.io_bytes(p) for p in probs)
     out["batched_512"] = {"tflops": fl / t / 1e12, "gbs": by / t / 1e9, "ms": 1e3 * t, "problems": 512,
                           "launches_per_run": plan.launches, "flop": fl, "bytes": by,
-                          "note": "one batched plan (grouped persistent launch + tensor-core launches), CUDA graph replay"}
+                          "note": "one batched plan (small problems in one grouped persistent launch, the others "
+                                  "as single launches over 4 worker streams), CUDA graph replay"}
     plan.close()
     del entries
     S, r = 192, 32
