@@ -64,6 +64,11 @@ CASES = [
     ([135, 19, 11], [1, 2, 3], 2, 40, False),     # inner 135, nq 19, partial K chunk
     ([37, 20, 30], [1, 2, 3], 1, 48, True),       # q = pi_1 with nq 37 (K-major tiles)
     ([21, 17, 300], [1, 3, 2], 1, 20, False),     # q = pi_1, nq 21, outer 5100
+    # inner <= 64: several slices share a 128-row tile (folded), last tile partly past the end
+    ([32, 40, 7], [1, 2, 3], 2, 32, True),        # inner 32: 4 slices per tile, 7 slices
+    ([64, 50, 9], [1, 2, 3], 2, 48, False),       # inner 64: 2 slices per tile
+    ([20, 33, 5], [1, 2, 3], 2, 40, True),        # inner 20 (unaligned: converters load), 32-row slots
+    ([48, 16, 11], [1, 2, 3], 2, 300, False),     # inner 48 in 64-row slots, two j blocks
 ]
 
 

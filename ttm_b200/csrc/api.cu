@@ -782,7 +782,7 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
     v.c = x.c;
     if (!tc_supported(v, TLIBTTM_PREC_BF16X3))
         return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm_ttm_f32_bf16x3_noalloc: shape not handled by the tensor-core "
-                                             "kernel (needs m > 16, and inner >= 32 or q = pi_1).");
+                                             "kernel (needs m > 16, and inner >= 17 or q = pi_1).");
     if (tc_image_bytes(v) > kNoAllocImageBytes)
         return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_f32_bf16x3_noalloc: B needs a " + std::to_string(tc_image_bytes(v)) +
                                          "-byte split image; this entry point holds at most " +

@@ -91,6 +91,8 @@ struct TcParams {
     float* c;
     const float* a;          // A itself, for the converters' own loads (ldg_a)
     int ldg_a;               // A rows not 16-byte aligned for TMA: the converters load A
+    int fold_kb;             // GEOM_MN with inner <= 64: slices per 128-row tile (1: unfolded)
+    int fold_ib_shift;       // log2 of the rows each slice takes in a folded tile (32 or 64)
     const uint8_t* bimg;     // pre-split B: [jb][kc][hi|lo][NT rows x 32 B]
     int* status;             // device status word (0 = ok)
     int64_t outer, nq, inner, m;
@@ -228,7 +230,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     issued[s] = (int)ph;
                     mbar_expect_tx(&a_full[s], L.a_bytes);
-                    if (GEOM == GEOM_MN) {
+                    if (GEOM == GEOM_MN && P.fold_kb > 1) {
+                        // folded tile: slices mt*KB .. +KB-1, the map ordered (i, k, l)
+                        tma_load_3d(a_at(s), &amap, &a_full[s], 0, (int)(mt * P.fold_kb), kc * kBK);
+                    } else if (GEOM == GEOM_MN) {
                         const int64_t k = mt / mper, ib = mt - k * mper;
                         tma_load_3d(a_at(s), &amap, &a_full[s], (int)(ib * kBM), kc * kBK, (int)k);
                     } else {
@@ -350,10 +355,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (GEOM == GEOM_MN) {
                         const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
                         if (have && P.ldg_a) {
-                            // elements (l, i .. i+3) of slice tk, zero outside A
-                            const int64_t gl = (int64_t)kc * kBK + l, i = r0 + w * 4;
-                            const float* src = P.a + (tk * P.nq + gl) * P.inner + i;
-                            const bool lv = gl < P.nq;
+                            // elements (l, i .. i+3) of slice tk (of slice tk * KB + row / IB when
+                            // folded), zero outside A
+                            const int64_t gl = (int64_t)kc * kBK + l;
+                            const int64_t sk = P.fold_kb > 1 ? mt * P.fold_kb + ((w * 4) >> P.fold_ib_shift) : tk;
+                            const int64_t i = P.fold_kb > 1 ? ((w * 4) & ((1 << P.fold_ib_shift) - 1)) : r0 + w * 4;
+                            const float* src = P.a + (sk * P.nq + gl) * P.inner + i;
+                            const bool lv = gl < P.nq && sk < P.outer;
                             x[it].x = (lv && i < P.inner) ? __ldg(src) : 0.0f;
                             x[it].y = (lv && i + 1 < P.inner) ? __ldg(src + 1) : 0.0f;
                             x[it].z = (lv && i + 2 < P.inner) ? __ldg(src + 2) : 0.0f;
@@ -413,7 +421,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_fence_after();
             const int64_t jb = t / P.tiles_m, mt = t - jb * P.tiles_m;
             int64_t k, r0;            // slice and first row (i for GEOM_MN, k for GEOM_K) of this warp
-            if (GEOM == GEOM_MN) {
+            if (GEOM == GEOM_MN && P.fold_kb > 1) {
+                // this warp's 32 rows lie in one slice of the folded tile
+                k = mt * P.fold_kb + ((q4 * 32) >> P.fold_ib_shift);
+                r0 = (q4 * 32) & ((1 << P.fold_ib_shift) - 1);
+            } else if (GEOM == GEOM_MN) {
                 k = mt / mper;
                 r0 = (mt - k * mper) * kBM + q4 * 32;
             } else {
@@ -428,7 +440,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tmem_ld32(tbase + (uint32_t)cc, v);
                 if (cc >= jleft) continue;
                 const int j0 = jb * P.nt + cc;
-                if (P.tma_c) {
+                if (P.tma_c && GEOM == GEOM_MN && k >= P.outer) {
+                    // folded last tile: this warp's slice lies past the end of C, nothing to store
+                } else if (P.tma_c) {
                     // Stage a 32 x 32 block in shared memory and store it with one TMA copy.
                     uint8_t* buf = stage0 + sb * kEpiBuf;
                     if (lane == 0) bulk_wait_read1();      // the copy that last read `buf` has finished reading it
@@ -456,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 } else {
                     // Direct stores (C rows not 16-byte aligned for a tensor map).
                     const int64_t r = r0 + lane;
-                    const bool rvalid = GEOM == GEOM_MN ? r < P.inner : r < P.outer;
+                    const bool rvalid = GEOM == GEOM_MN ? (r < P.inner && k < P.outer) : r < P.outer;
                     if (rvalid) {
                         float* p = GEOM == GEOM_MN ? P.c + (k * P.m + j0) * P.inner + r : P.c + r * P.m + j0;
                         const int64_t cs = GEOM == GEOM_MN ? P.inner : 1;
@@ -950,6 +964,22 @@ bool encode_a_map(const View3& v, int geom, CUtensorMap* map)
     return r == CUDA_SUCCESS;
 }
 
+// A of a folded GEOM_MN tile as the 3-D map (i, k, l) -- dimensions deliberately not in stride
+// order -- with boxes of ib i x kb slices x kBK l, which land in shared memory as [l][kb*ib rows]:
+// the same layout as an unfolded tile of 128 i.
+bool encode_a_map_folded(const View3& v, int ib, int kb, CUtensorMap* map)
+{
+    EncodeTiledFn cuTensorMapEncodeTiled = encode_fn();
+    if (!cuTensorMapEncodeTiled) return false;
+    cuuint64_t dims[3] = {(cuuint64_t)v.inner, (cuuint64_t)v.outer, (cuuint64_t)v.nq};
+    cuuint64_t strides[2] = {(cuuint64_t)(v.inner * v.nq) * 4, (cuuint64_t)v.inner * 4};
+    cuuint32_t box[3] = {(cuuint32_t)ib, (cuuint32_t)kb, (cuuint32_t)kBK};
+    cuuint32_t es[3] = {1, 1, 1};
+    return cuTensorMapEncodeTiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void*>(v.a), dims, strides, box, es,
+                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // C as a tensor map for the TMA-store epilogue: 32 x 32 boxes. False when C's rows are not
 // 16-byte aligned (the epilogue then stores directly).
 bool encode_c_map(const View3& v, int geom, CUtensorMap* map)
@@ -1000,8 +1030,17 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     TcParams P{};
     P.ldg_a = tma_a_ok(v, geom) ? 0 : 1;
     P.a = static_cast<const float*>(v.a);
+    // inner <= 64: KB = 128 / IB slices share a 128-row tile (IB = 32 or 64 rows each)
+    P.fold_kb = 1;
+    P.fold_ib_shift = 7;
+    if (geom == GEOM_MN && v.inner <= 64) {
+        P.fold_ib_shift = v.inner <= 32 ? 5 : 6;
+        P.fold_kb = kBM >> P.fold_ib_shift;
+    }
+    if (!P.ldg_a && !(P.fold_kb > 1 ? encode_a_map_folded(v, 1 << P.fold_ib_shift, P.fold_kb, &amap)
+                                    : encode_a_map(v, geom, &amap)))
+        P.ldg_a = 1;   // the driver declined the map: the converters load A
     if (P.ldg_a) std::memset(&amap, 0, sizeof(amap));
-    else if (!encode_a_map(v, geom, &amap)) return cudaErrorInvalidValue;
     P.tma_c = encode_c_map(v, geom, &cmap) ? 1 : 0;
     if (!P.tma_c) std::memset(&cmap, 0, sizeof(cmap));
     P.c = static_cast<float*>(v.c);
@@ -1011,7 +1050,9 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     P.nq = v.nq;
     P.inner = v.inner;
     P.m = v.m;
-    P.tiles_m = geom == GEOM_MN ? v.outer * ((v.inner + kBM - 1) / kBM) : (v.outer + kBM - 1) / kBM;
+    P.tiles_m = geom == GEOM_MN ? (P.fold_kb > 1 ? (v.outer + P.fold_kb - 1) / P.fold_kb
+                                                 : v.outer * ((v.inner + kBM - 1) / kBM))
+                                : (v.outer + kBM - 1) / kBM;
     P.tiles = P.tiles_m * jblocks;
     P.nt = nt;
     P.jblocks = jblocks;
@@ -1380,7 +1421,7 @@ bool tc_supported(const View3& v, int precision)
     if (v.m <= kSmallM) return false;
     const int g = geometry_of(v);
     if ((reinterpret_cast<uintptr_t>(v.a) & 3u) != 0) return false;   // float-aligned A
-    if (g == GEOM_MN && v.inner < 32) return false;
+    if (g == GEOM_MN && v.inner < 17) return false;   // a folded tile gives each slice >= 32 rows
     // TMA coordinates are signed 32-bit.
     if (v.outer >= (int64_t(1) << 31) || v.nq >= (int64_t(1) << 31) || v.inner >= (int64_t(1) << 31)) return false;
     return true;
