@@ -201,12 +201,14 @@ typedef struct tlibttm_problem {
 } tlibttm_problem;
 
 /*
- * Batched plan: `count` independent TTMs of one dtype. Dense problems on the
- * SIMT paths run in ONE persistent grouped launch whose blocks pull work items
- * (slice-GEMM tiles or row blocks of small-m problems, largest problems first)
- * from a device work queue; problems that take the tensor-core path
- * (precision bf16x3/auto) or that have non-dense strides are launched after it
- * on the same stream. Errors name the offending problem ("problem 7: ...").
+ * Batched plan: `count` independent TTMs of one dtype. Small dense problems run
+ * in ONE persistent grouped launch whose blocks pull work items (slice-GEMM tiles
+ * or row blocks of small-m problems, largest problems first) from a device work
+ * queue. Problems of at least 2^18 elements of A (tensor-core ones under
+ * precision bf16x3/auto, small-m ones always) and problems with non-dense strides
+ * get their own launch of the kernel the planner picks; these run largest first
+ * on worker streams the plan owns, forked from `stream` and joined back into it.
+ * Errors name the offending problem ("problem 7: ...").
  */
 int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_problem* problems,
                          tlibttm_plan** plan);
