@@ -203,11 +203,15 @@ def test_stream_rows_contiguous_fibres(cuda, oracle_c, dtype):
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_short_contiguous_fibres(cuda, oracle_c, dtype):
-    """q = pi_1 with n_q <= 16: rows of A are short and contiguous (the flat-tile row kernel);
-    row counts that are not multiples of a warp's tile, n_q = 1, every m bucket, both B layouts."""
+    """q = pi_1 with n_q <= 16: rows of A are short and contiguous (the span and flat-tile row
+    kernels); row counts that are not multiples of a span or a warp's tile, n_q = 1, every m bucket,
+    both B layouts."""
     rng = np.random.default_rng(31)
+    # n_q in {1, 2, 4, 8, 16}: the span kernel (tail spans, m below its bucket, vector and scalar
+    # stores); other lengths: the flat-tile kernel
     for n, (nq, outer, m) in enumerate(((1, 5000, 1), (2, 70001, 8), (3, 4099, 3), (5, 12345, 16), (16, 33333, 2),
-                                        (16, 31, 5), (7, 100000, 1))):
+                                        (16, 31, 5), (7, 100000, 1), (4, 9999, 4), (8, 777, 16), (4, 100003, 1),
+                                        (8, 5001, 3), (1, 333, 16))):
         na = [nq, outer]
         pia = [1, 2]
         nc = [m, outer]

@@ -537,6 +537,81 @@ __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
 }
 
 // ---------------------------------------------------------------------------------------------
+// rowspan: small m, contiguous fibres of NQ in {1, 2, 4, 8, 16} elements (at most a span), A
+// 16-byte aligned. Thread t reads the 64-byte span (16 floats / 8 doubles) holding the R = span /
+// NQ whole fibres t*R .. t*R + R-1 with 128-bit loads: consecutive threads read consecutive
+// spans, so a warp's loads are fully coalesced and nothing is staged. Its R*m outputs are
+// contiguous in C. B sits in shared memory (broadcast reads). Used where a thread's outputs take
+// at most 64 bytes (measured: more outputs per thread scatter the stores too widely).
+// ---------------------------------------------------------------------------------------------
+template <typename T, int MB, int NQ>
+__global__ void __launch_bounds__(256) rowspan_kernel(View3 v)
+{
+    constexpr int E = 64 / (int)sizeof(T), R = E / NQ, VW = 16 / (int)sizeof(T), NV = E / VW;
+    static_assert(NQ <= E, "a fibre fits a span");
+    __shared__ T bs[NQ * MB];
+    const T* __restrict__ B = static_cast<const T*>(v.b);
+    for (int e = threadIdx.x; e < NQ * MB; e += blockDim.x) {
+        const int l = e / MB, j = e - l * MB;
+        bs[e] = j < v.m ? (v.b_cm ? B[j + (int64_t)l * v.m] : B[(int64_t)j * NQ + l]) : T(0);
+    }
+    __syncthreads();
+    const T* __restrict__ A = static_cast<const T*>(v.a);
+    T* __restrict__ Cp = static_cast<T*>(v.c);
+    const int64_t rows = v.outer, spans = (rows + R - 1) / R;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < spans; t += stride) {
+        const int64_t r0 = t * R;
+        T a[E];
+        if (r0 + R <= rows) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) {
+                T x[VW];
+                load_vec<T, VW>(x, A + r0 * NQ + q * VW);
+#pragma unroll
+                for (int w = 0; w < VW; ++w) a[q * VW + w] = x[w];
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < E; ++e) a[e] = (r0 + e / NQ < rows) ? __ldg(A + r0 * NQ + e) : T(0);
+        }
+        T* cp = Cp + r0 * v.m;
+        // R*m contiguous outputs: with m == MB, a 16-byte aligned C and R*MB a multiple of VW,
+        // written VW at a time (a vector covers MB / VW of a row, or VW / MB rows)
+        const bool vec = r0 + R <= rows && v.m == MB && (R * MB) % VW == 0 &&
+                         (reinterpret_cast<uintptr_t>(cp) & 15u) == 0;
+        if (vec) {
+#pragma unroll
+            for (int q = 0; q < R * MB / VW; ++q) {
+                T x[VW];
+#pragma unroll
+                for (int w = 0; w < VW; ++w) {
+                    const int o = q * VW + w, r = o / MB, j = o - r * MB;
+                    T acc = T(0);
+#pragma unroll
+                    for (int l = 0; l < NQ; ++l) acc = fma_t(a[r * NQ + l], bs[l * MB + j], acc);
+                    x[w] = acc;
+                }
+                store_vec<T, VW>(cp + q * VW, x);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (r0 + r >= rows) break;
+#pragma unroll
+                for (int j = 0; j < MB; ++j) {
+                    if (j >= v.m) break;
+                    T acc = T(0);
+#pragma unroll
+                    for (int l = 0; l < NQ; ++l) acc = fma_t(a[r * NQ + l], bs[l * MB + j], acc);
+                    cp[(int64_t)r * v.m + j] = acc;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // strided: one thread per C element, strides taken from the caller.
 // ---------------------------------------------------------------------------------------------
 template <typename T>
@@ -726,9 +801,36 @@ cudaError_t rowflat_launch(const View3& v, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <typename T, int NQ>
+cudaError_t rowspan_launch(const View3& v, cudaStream_t s)
+{
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t spans = ceil_div(v.outer, (int64_t)(64 / sizeof(T) / NQ));
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(spans, 256), (int64_t)sms * 16));
+    if (v.m <= 1) rowspan_kernel<T, 1, NQ><<<blocks, 256, 0, s>>>(v);
+    else if (v.m <= 2) rowspan_kernel<T, 2, NQ><<<blocks, 256, 0, s>>>(v);
+    else if (v.m <= 4) rowspan_kernel<T, 4, NQ><<<blocks, 256, 0, s>>>(v);
+    else if (v.m <= 8) rowspan_kernel<T, 8, NQ><<<blocks, 256, 0, s>>>(v);
+    else rowspan_kernel<T, 16, NQ><<<blocks, 256, 0, s>>>(v);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t rowdot_dispatch(const View3& v, cudaStream_t s)
 {
+    const int64_t span = 64 / (int64_t)sizeof(T);
+    const int64_t mb = v.m <= 1 ? 1 : v.m <= 2 ? 2 : v.m <= 4 ? 4 : v.m <= 8 ? 8 : 16;
+    if (aligned16(v.a) && v.nq <= span && (span / v.nq) * mb * (int64_t)sizeof(T) <= 64) {
+        switch (v.nq) {
+        case 1: return rowspan_launch<T, 1>(v, s);
+        case 2: return rowspan_launch<T, 2>(v, s);
+        case 4: return rowspan_launch<T, 4>(v, s);
+        case 8: return rowspan_launch<T, 8>(v, s);
+        case 16: if constexpr (sizeof(T) == 4) return rowspan_launch<T, 16>(v, s); break;
+        default: break;
+        }
+    }
     if (v.nq <= kFlatMaxNq) {
         if (v.m <= 1) return rowflat_launch<T, 1>(v, s);
         if (v.m <= 2) return rowflat_launch<T, 2>(v, s);
