@@ -587,12 +587,14 @@ struct StreamGeom {
     static constexpr int LB = (int)(SB / (P * sizeof(T)));             // l per stage
 };
 
-// The kernel comes in two builds: 112 registers per thread (two CTAs of 288 threads per SM) and
-// a lean 72 (three CTAs per SM), which fits without spills for m <= 4, and m <= 8 in float.
-constexpr bool stream_lean_ok(int mb, size_t es) { return mb <= 4 || (mb <= 8 && es == 4); }
+// The kernel comes in two builds by resident CTAs per SM (CPS). A warp's registers come from
+// its sub-partition's quarter of the register file (16384), and the nine warps of CPS CTAs spread
+// over the four sub-partitions, so the per-thread cap is 16384 / ceil(9 CPS / 4) / 32 rounded
+// down to 8: 96 for two CTAs (no spills for m <= 8), 168 for one (any m <= 16).
+constexpr int stream_nreg(int cps) { return cps == 2 ? 96 : 168; }
 
-template <typename T, int MB, bool ROWS, bool LEAN>
-__global__ void __maxnreg__(LEAN ? 72 : 112)
+template <typename T, int MB, bool ROWS, int CPS>
+__global__ void __maxnreg__(stream_nreg(CPS))
     stream_cols_kernel(const __grid_constant__ CUtensorMap amap, StreamParams P)
 {
     using G = StreamGeom<T, ROWS>;
@@ -679,13 +681,24 @@ __global__ void __maxnreg__(LEAN ? 72 : 112)
             const int64_t kb = t / mper, ib = t - kb * mper;
             const int kc0 = r * P.kper, kc1 = min(kc0 + P.kper, P.kchunks);
             if (r != staged) {
-                // stage rows [kc0 * lb, kc1 * lb) of B: bs[l][j] = B(j, l), zero outside B
+                // stage rows [kc0 * lb, kc1 * lb) of B: bs[l][j] = B(j, l), zero outside B. The
+                // loads go out four at a time ahead of their stores: bs is a generic pointer, so
+                // the compiler would otherwise wait for each load before the next store.
                 asm volatile("bar.sync 1, 256;" ::: "memory");
-                const int rows = (kc1 - kc0) * P.lb;
-                for (int e = tid; e < rows * MB; e += 256) {
-                    const int lr = e / MB, j = e - lr * MB;
-                    const int64_t l = (int64_t)kc0 * P.lb + lr;
-                    bs[e] = (j < P.m && l < P.nq) ? (P.b_cm ? Bg[j + l * P.m] : Bg[j * P.nq + l]) : T(0);
+                const int total = (kc1 - kc0) * P.lb * MB;
+                for (int e0 = tid; e0 < total; e0 += 256 * 4) {
+                    T v[4];
+#pragma unroll
+                    for (int x = 0; x < 4; ++x) {
+                        const int e = e0 + x * 256;
+                        const int lr = e / MB, j = e - lr * MB;
+                        const int64_t l = (int64_t)kc0 * P.lb + lr;
+                        v[x] = (e < total && j < P.m && l < P.nq)
+                                   ? __ldg(P.b_cm ? Bg + j + l * P.m : Bg + j * P.nq + l) : T(0);
+                    }
+#pragma unroll
+                    for (int x = 0; x < 4; ++x)
+                        if (e0 + x * 256 < total) bs[e0 + x * 256] = v[x];
                 }
                 asm volatile("bar.sync 1, 256;" ::: "memory");
                 staged = r;
@@ -794,6 +807,22 @@ __global__ void __maxnreg__(LEAN ? 72 : 112)
                         for (int w = 0; w < 2; ++w)
                             if (kr[w] < P.outer) {
                                 T* cp = C + kr[w] * P.m;
+                                if constexpr (MB * sizeof(T) % 16 == 0) {
+                                    // whole rows of MB outputs on 16-byte boundaries: vector stores
+                                    if (P.m == MB && (reinterpret_cast<uintptr_t>(C) & 15u) == 0) {
+                                        using V16 = typename V16Tc<T>::type;
+                                        constexpr int EPC = 16 / (int)sizeof(T);
+#pragma unroll
+                                        for (int q = 0; q < MB / EPC; ++q) {
+                                            V16 v;
+                                            T* vv = reinterpret_cast<T*>(&v);
+#pragma unroll
+                                            for (int f = 0; f < EPC; ++f) vv[f] = acc[w][q * EPC + f];
+                                            *reinterpret_cast<V16*>(cp + q * EPC) = v;
+                                        }
+                                        continue;
+                                    }
+                                }
 #pragma unroll
                                 for (int j = 0; j < MB; ++j)
                                     if (j < P.m) cp[j] = acc[w][j];
@@ -1110,8 +1139,8 @@ bool encode_stream_map(const View3& v, int dtype, int ib, int h, int kb, CUtenso
 }
 
 // cudaFuncSetAttribute once per kernel instance and device (devices 0..63): the full dynamic
-// shared memory, and for instances meant to run three CTAs per SM the largest shared-memory
-// carveout (three CTAs of ~74 KB).
+// shared memory and, when asked, the largest shared-memory carveout (so that two CTAs of
+// ~113 KB fit on one SM).
 template <typename K>
 cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done, bool max_carveout = false)
 {
@@ -1124,36 +1153,38 @@ cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done, bool
     return e;
 }
 
-template <typename T, int MB, bool ROWS, bool LEAN>
+template <typename T, int MB, bool ROWS, int CPS>
 cudaError_t launch_stream_mb(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
                              cudaStream_t s)
 {
     static std::atomic<uint64_t> done{0};
-    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS, LEAN>, dev, done, LEAN);
+    // the whole unified L1 as shared memory, so that CPS rings fit side by side
+    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS, CPS>, dev, done, true);
     if (e != cudaSuccess) return e;
-    stream_cols_kernel<T, MB, ROWS, LEAN><<<grid, kStreamThreads, smem, s>>>(amap, P);
+    stream_cols_kernel<T, MB, ROWS, CPS><<<grid, kStreamThreads, smem, s>>>(amap, P);
     return cudaGetLastError();
 }
 
+// The build for `cps` CTAs per SM: two for m <= 8, one for any m.
 template <typename T, int MB, bool ROWS>
-cudaError_t launch_stream_lean(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
-                               bool lean, cudaStream_t s)
+cudaError_t launch_stream_cps(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
+                              int cps, cudaStream_t s)
 {
-    if constexpr (MB <= 4 || (MB <= 8 && sizeof(T) == 4)) {
-        if (lean) return launch_stream_mb<T, MB, ROWS, true>(amap, P, smem, grid, dev, s);
+    if constexpr (MB <= 8) {
+        if (cps == 2) return launch_stream_mb<T, MB, ROWS, 2>(amap, P, smem, grid, dev, s);
     }
-    return launch_stream_mb<T, MB, ROWS, false>(amap, P, smem, grid, dev, s);
+    return launch_stream_mb<T, MB, ROWS, 1>(amap, P, smem, grid, dev, s);
 }
 
 template <typename T, bool ROWS>
 cudaError_t launch_stream_t(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
-                            bool lean, cudaStream_t s)
+                            int cps, cudaStream_t s)
 {
-    if (P.m <= 1) return launch_stream_lean<T, 1, ROWS>(amap, P, smem, grid, dev, lean, s);
-    if (P.m <= 2) return launch_stream_lean<T, 2, ROWS>(amap, P, smem, grid, dev, lean, s);
-    if (P.m <= 4) return launch_stream_lean<T, 4, ROWS>(amap, P, smem, grid, dev, lean, s);
-    if (P.m <= 8) return launch_stream_lean<T, 8, ROWS>(amap, P, smem, grid, dev, lean, s);
-    return launch_stream_lean<T, 16, ROWS>(amap, P, smem, grid, dev, lean, s);
+    if (P.m <= 1) return launch_stream_cps<T, 1, ROWS>(amap, P, smem, grid, dev, cps, s);
+    if (P.m <= 2) return launch_stream_cps<T, 2, ROWS>(amap, P, smem, grid, dev, cps, s);
+    if (P.m <= 4) return launch_stream_cps<T, 4, ROWS>(amap, P, smem, grid, dev, cps, s);
+    if (P.m <= 8) return launch_stream_cps<T, 8, ROWS>(amap, P, smem, grid, dev, cps, s);
+    return launch_stream_cps<T, 16, ROWS>(amap, P, smem, grid, dev, cps, s);
 }
 
 // Row mode: A as the 2-D tensor map (l, row) of its contiguous fibres, boxes of LB l (64 bytes) x
@@ -1174,7 +1205,7 @@ bool encode_rows_map(const View3& v, int dtype, CUtensorMap* map)
     return r == CUDA_SUCCESS;
 }
 
-// Launch geometry of the TMA-fed small-m kernel (two CTAs per SM): box shape, ring depth, the
+// Launch geometry of the TMA-fed small-m kernel (one or two CTAs per SM): box shape, ring depth, the
 // l split and the dynamic shared memory (ring + staged rows of B + barriers).
 struct StreamShape {
     bool rows;
@@ -1261,18 +1292,18 @@ bool stream_split(const View3& v, size_t es, int NP, int LB, int sms, StreamShap
 {
     sh.lb = (int)std::min<int64_t>(LB, v.nq);
     sh.kchunks = (int)((v.nq + sh.lb - 1) / sh.lb);
-    // per CTA: two or three CTAs per SM share its 228 KB of shared memory (1 KB each reserved).
-    // Three (the lean build, m = 3..8) only when the tiles alone leave CTA slots of two per SM
-    // empty: measured, the smaller ring and B stage of three CTAs cost more than the extra warps
-    // gain when there are tiles enough, or when m <= 2 keeps the consumers light.
-    sh.per_sm = (stream_lean_ok(sh.mb, es) && sh.mb >= 4 && sh.tiles < 2 * (int64_t)sms) ? 3 : 2;
-    const size_t budget = (sh.per_sm == 3 ? 74 : 112) * 1024 - 1024 - 256;
+    // CTAs per SM (one or two share its 228 KB of shared memory, 1 KB each reserved) and the ring
+    // of each, measured over the layout/mode sweep: row mode, m > 8 and column mode with fewer
+    // tiles than SMs run one CTA (168 registers) with a 128 KB ring; other column-mode shapes two
+    // (96 registers) with 48 KB rings. More bytes in flight per SM than that slowed the
+    // write-heavy short-n_q cases; three CTAs of 72 registers lost to both.
+    sh.per_sm = (sh.rows || sh.mb > 8 || sh.tiles < (int64_t)sms) ? 1 : 2;
+    const size_t budget = (sh.per_sm == 2 ? 112 : 227) * 1024 - 1024 - 256;
     const size_t row = (size_t)sh.lb * sh.mb * es;   // staged B bytes per l chunk
-    // ring per CTA (192 KB in flight per SM either way): two CTAs 96 KB when B fits beside it,
-    // down to 64 KB, otherwise 80 KB; three CTAs 64 KB down to 48 KB, otherwise 48 KB; B staged
-    // a part at a time when it does not fit; at least two stages
-    const size_t hi = sh.per_sm == 3 ? 64 * 1024 : 96 * 1024, lo = sh.per_sm == 3 ? 48 * 1024 : 64 * 1024,
-                 fb = sh.per_sm == 3 ? 48 * 1024 : 80 * 1024;
+    // ring per CTA from hi down to lo while B fits beside it, otherwise fb with B staged a part
+    // at a time; at least two stages
+    const size_t hi = sh.per_sm == 2 ? 48 * 1024 : 128 * 1024, lo = sh.per_sm == 2 ? 32 * 1024 : 96 * 1024,
+                 fb = sh.per_sm == 2 ? 48 * 1024 : 128 * 1024;
     int kper_max = 0;
     sh.stages = 0;
     for (int st = std::max<int>(2, (int)(hi / sh.sb)); st >= std::max<int>(2, (int)(lo / sh.sb)); --st)
@@ -1397,11 +1428,11 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
     }
     const int grid = (int)std::min<int64_t>(sh.units, (int64_t)g_sm_count * sh.per_sm);
     if (e == cudaSuccess) {
-        const bool lean = sh.per_sm == 3;
-        e = sh.rows ? (dtype == 0 ? launch_stream_t<float, true>(amap, P, sh.smem, grid, dev, lean, s)
-                                  : launch_stream_t<double, true>(amap, P, sh.smem, grid, dev, lean, s))
-                    : (dtype == 0 ? launch_stream_t<float, false>(amap, P, sh.smem, grid, dev, lean, s)
-                                  : launch_stream_t<double, false>(amap, P, sh.smem, grid, dev, lean, s));
+        const int cps = sh.per_sm;
+        e = sh.rows ? (dtype == 0 ? launch_stream_t<float, true>(amap, P, sh.smem, grid, dev, cps, s)
+                                  : launch_stream_t<double, true>(amap, P, sh.smem, grid, dev, cps, s))
+                    : (dtype == 0 ? launch_stream_t<float, false>(amap, P, sh.smem, grid, dev, cps, s)
+                                  : launch_stream_t<double, false>(amap, P, sh.smem, grid, dev, cps, s));
     }
     if (scratch) cudaFreeAsync(scratch, s);
     return e;
