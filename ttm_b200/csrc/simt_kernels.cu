@@ -15,6 +15,7 @@
 //
 // All index arithmetic is 64-bit (a 256^4 tensor has 2^32 elements).
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -58,6 +59,21 @@ __device__ __forceinline__ void store_vec(T* p, const T (&r)[W])
 
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Packed FP32 pairs (sm_100): d = a * b + d lane by lane, each lane one correctly rounded fused
+// multiply-add like fmaf, two per instruction. Pairs live in 64-bit registers, low half first.
+__device__ __forceinline__ void ffma2(unsigned long long& d, unsigned long long a, unsigned long long b)
+{
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+__device__ __forceinline__ unsigned long long pair_dup(float x)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float pair_lo(unsigned long long r) { return __uint_as_float((unsigned)r); }
+__device__ __forceinline__ float pair_hi(unsigned long long r) { return __uint_as_float((unsigned)(r >> 32)); }
 
 // ---------------------------------------------------------------------------------------------
 // simt_gemm
@@ -165,11 +181,21 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
         }
     };
 
+    // FP32 accumulates in packed column pairs (acc2[i][j / 2], column j in the low half when j
+    // is even): half the FMA instructions of one per output
+    constexpr bool PK = std::is_same<T, float>::value;
     T acc[TM][TN];
+    unsigned long long acc2[PK ? TM : 1][PK ? TN / 2 : 1];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+    if constexpr (PK) {
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < TN / 2; ++j) acc2[i][j] = 0ull;
+    }
 
     const int64_t nk = ceil_div(nq, BK);
     load_tiles(0);
@@ -181,6 +207,21 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
         if (kt + 1 < nk) load_tiles((kt + 1) * BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
+            if constexpr (PK) {
+                const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * RV]);
+                const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][BM / 2 + ty * RV]);
+                const ulonglong2 b0 = *reinterpret_cast<const ulonglong2*>(&Bs[buf][kk][tx * RV]);
+                const ulonglong2 b1 = *reinterpret_cast<const ulonglong2*>(&Bs[buf][kk][BN / 2 + tx * RV]);
+                const unsigned long long bp[TN / 2] = {b0.x, b0.y, b1.x, b1.y};
+                const float af[TM] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+                for (int i = 0; i < TM; ++i) {
+                    const unsigned long long ap = pair_dup(af[i]);
+#pragma unroll
+                    for (int j = 0; j < TN / 2; ++j) ffma2(acc2[i][j], ap, bp[j]);
+                }
+                continue;
+            }
             T af[TM], bf[TN];
             typedef typename V16<T>::type VT;
             VT a0 = *reinterpret_cast<const VT*>(&As[buf][kk][ty * RV]);
@@ -201,6 +242,16 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
         }
         if (kt + 1 < nk) store_tiles(buf ^ 1);
         __syncthreads();
+    }
+
+    if constexpr (PK) {
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < TN / 2; ++j) {
+                acc[i][2 * j] = pair_lo(acc2[i][j]);
+                acc[i][2 * j + 1] = pair_hi(acc2[i][j]);
+            }
     }
 
     // Epilogue: C(row, j) = cbase(row) + j*inner, cbase = (row/inner)*inner*m + row%inner.
@@ -263,8 +314,10 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
     }
 }
 
+// Two CTAs per SM: at most 128 registers a thread (16 warps of 128 fill each sub-partition's
+// quarter of the register file).
 template <typename T, bool AK, bool VEC, bool BCM>
-__global__ void __launch_bounds__(256) simt_gemm_kernel(View3 v)
+__global__ void __launch_bounds__(256, 2) simt_gemm_kernel(View3 v)
 {
     constexpr int RV = 16 / sizeof(T);
     __shared__ GemmSmem<T> sm;
