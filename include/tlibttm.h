@@ -117,7 +117,7 @@ int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p,
  * Limits: a, b and c must all be device memory of the current device (no host
  * staging); A and C dense under their layout; m > 16 and either inner >= 17
  * or q == pia[0]; and the B image,
- * ceil(m/16)*16 * ceil(n_q/16)*16 * 4 bytes, at most 1 MiB (for example
+ * ceil(m/16)*16 * ceil(n_q/32)*32 * 4 bytes, at most 1 MiB (for example
  * m = 256 with n_q <= 1024). Larger or unsupported problems are rejected with
  * TLIBTTM_ERR_ARG / TLIBTTM_ERR_UNSUPPORTED and a message; nothing is launched.
  *

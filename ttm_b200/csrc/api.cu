@@ -787,7 +787,7 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
         return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_f32_bf16x3_noalloc: B needs a " + std::to_string(tc_image_bytes(v)) +
                                          "-byte split image; this entry point holds at most " +
                                          std::to_string(kNoAllocImageBytes) +
-                                         " bytes (ceil(m/16)*16 * ceil(n_q/16)*16 * 4 bytes, e.g. m = 256 with n_q <= 1024).");
+                                         " bytes (ceil(m/16)*16 * ceil(n_q/32)*32 * 4 bytes, e.g. m = 256 with n_q <= 1024).");
     int kid = K_NONE;
     e = launch_tc_noalloc(v, static_cast<cudaStream_t>(stream), &kid);
     if (e == cudaSuccess) ++g_launches;   // split_b_kernel; note_launch counts the main kernel

@@ -6,6 +6,23 @@
 
 namespace tlibttm {
 
+#ifdef __CUDACC__
+// Packed FP32 pairs (sm_100): d = a * b + d lane by lane, each lane one correctly rounded fused
+// multiply-add like fmaf, two per instruction. Pairs live in 64-bit registers, low half first.
+static __device__ __forceinline__ void ffma2(unsigned long long& d, unsigned long long a, unsigned long long b)
+{
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+static __device__ __forceinline__ unsigned long long pair_dup(float x)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(x));
+    return r;
+}
+static __device__ __forceinline__ float pair_lo(unsigned long long r) { return __uint_as_float((unsigned)r); }
+static __device__ __forceinline__ float pair_hi(unsigned long long r) { return __uint_as_float((unsigned)(r >> 32)); }
+#endif
+
 // Dense slice view of one mode-q TTM.
 //
 // With qhat = pi^{-1}(q) (one-based position of q in A's layout pi), a tensor

@@ -60,20 +60,6 @@ __device__ __forceinline__ void store_vec(T* p, const T (&r)[W])
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
 
-// Packed FP32 pairs (sm_100): d = a * b + d lane by lane, each lane one correctly rounded fused
-// multiply-add like fmaf, two per instruction. Pairs live in 64-bit registers, low half first.
-__device__ __forceinline__ void ffma2(unsigned long long& d, unsigned long long a, unsigned long long b)
-{
-    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
-}
-__device__ __forceinline__ unsigned long long pair_dup(float x)
-{
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(x));
-    return r;
-}
-__device__ __forceinline__ float pair_lo(unsigned long long r) { return __uint_as_float((unsigned)r); }
-__device__ __forceinline__ float pair_hi(unsigned long long r) { return __uint_as_float((unsigned)(r >> 32)); }
 
 // ---------------------------------------------------------------------------------------------
 // simt_gemm

@@ -12,14 +12,14 @@
 //   GEOM_K  (inner == 1, the contraction mode is the fastest): MMA rows are
 //            128 consecutive k; A's tile is K-major; TMA box (32 l, 128 k).
 // MMA shape M = 128, N = NT (<= 256, the rows of B in this tile), K = 16 per
-// instruction, 32 l per pipeline stage.
+// instruction, 32 l (two sub-blocks of 16, six MMAs) per pipeline stage.
 //
-// Warp roles (320 threads, one CTA per SM, persistent over tiles):
-//   warp 0     TMA producer: FP32 A tile (tensor map) + the pre-split B_hi/B_lo
-//              image of this K chunk (bulk copy) into stage s.
+// Warp roles (480 threads, one CTA per SM, persistent over tiles):
+//   warp 0     TMA producer of the FP32 A tile (tensor map).
 //   warp 1     TMEM allocator and MMA issuer (one elected lane).
-//   warps 2-5  converters: FP32 tile -> bf16 hi/lo in the swizzled UMMA layout.
-//   warps 6-9  epilogue: TMEM -> registers -> global C (double-buffered accumulator).
+//   warp 2     bulk copies of the pre-split B_hi/B_lo image of this stage.
+//   warps 3-10 converters: FP32 tile -> bf16 hi/lo in the swizzled UMMA layout.
+//   warps 11-14 epilogue: TMEM -> registers -> global C (double-buffered accumulator).
 // Every mbarrier wait is bounded (4 s of %globaltimer); on expiry the CTA raises
 // an abort flag, records an error in the device status word, drains its own
 // bulk copies, frees TMEM and returns.
@@ -46,7 +46,8 @@ constexpr int kGroupWarps = kConvWarps / kConvGroups;
 constexpr int kThreads = (3 + kConvWarps + 4) * 32;  // A producer, MMA, B producer, converters, 4 epilogue warps
 constexpr int kConvThreads = kConvWarps * 32;
 constexpr int kBM = 128;       // MMA M
-constexpr int kBK = 16;        // l per stage (one MMA K step)
+constexpr int kBK = 16;        // l per sub-block (one MMA K step)
+constexpr int kSub = 2;        // sub-blocks per pipeline stage: 3 * kSub MMAs per barrier round
 constexpr int kMaxNT = 256;    // MMA N max
 
 enum { GEOM_MN = 0, GEOM_K = 1 };
@@ -100,29 +101,32 @@ struct TcParams {
     int64_t tiles;           // total tiles
     int nt;                  // MMA N (multiple of 16, <= 256)
     int jblocks;
-    int kchunks;
+    int kchunks;             // 16-l sub-blocks of n_q
+    int kstages;             // pipeline stages per tile: ceil(kchunks / kSub)
     int fstages;             // A ring depth (FP32 tile, converted in place)
     int ostages;             // B ring depth
     int tma_c;               // epilogue stores C through the C tensor map
 };
 
-// Shared memory: [A ring: FP32 tile, converted in place to bf16 hi|lo][B ring: B_hi|B_lo]
-//                [epilogue staging][barriers].
+// Shared memory: [A ring][B ring][epilogue staging][barriers]. An A stage holds kSub FP32
+// sub-blocks of 128 rows x 16 l, each converted in place to [bf16 hi | bf16 lo]; a B stage holds
+// [hi | lo] of each sub-block's 16 l of B.
 struct SmemLayout {
-    uint32_t a_bytes, abf_bytes, b_bytes, bstage_bytes;
+    uint32_t a_bytes, asub_bytes, abf_bytes, b_bytes, bstage_bytes;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int nt)
 {
     SmemLayout L;
-    L.a_bytes = kBM * kBK * 4;              // 8 KB FP32 tile (its bf16 hi and lo halves after conversion)
+    L.asub_bytes = kBM * kBK * 4;           // 8 KB FP32 sub-block (its bf16 hi and lo halves after conversion)
+    L.a_bytes = kSub * L.asub_bytes;
     L.abf_bytes = kBM * kBK * 2;            // 4 KB per bf16 part
-    L.b_bytes = (uint32_t)nt * kBK * 2;     // per part, multiple of 512
-    L.bstage_bytes = 2 * L.b_bytes;
+    L.b_bytes = (uint32_t)nt * kBK * 2;     // per part and sub-block, multiple of 512
+    L.bstage_bytes = kSub * 2 * L.b_bytes;
     return L;
 }
 
-constexpr int kMaxA = 24, kMaxB = 4;
+constexpr int kMaxA = 12, kMaxB = 3;
 constexpr uint32_t kEpiBuf = 32 * 32 * 4;        // one 32 x 32 fp32 staging tile
 constexpr uint32_t kEpiBytes = 4 * 2 * kEpiBuf;  // 4 epilogue warps, double-buffered
 constexpr size_t kCtrlBytes = 1024;
@@ -134,8 +138,8 @@ __host__ inline bool choose_stages(int nt, int& as, int& bs, size_t& smem)
     const SmemLayout L = smem_layout(nt);
     const size_t avail = kSmemBudget - 1024 - kCtrlBytes - kEpiBytes;
     bs = kMaxB;
-    while (bs > 2 && (size_t)bs * L.bstage_bytes + 8 * L.a_bytes > avail) --bs;
-    if ((size_t)bs * L.bstage_bytes + 8 * L.a_bytes > avail) return false;
+    while (bs > 2 && (size_t)bs * L.bstage_bytes + 4 * L.a_bytes > avail) --bs;
+    if ((size_t)bs * L.bstage_bytes + 4 * L.a_bytes > avail) return false;
     as = (int)((avail - (size_t)bs * L.bstage_bytes) / L.a_bytes);
     if (as > kMaxA) as = kMaxA;
     smem = 1024 + (size_t)as * L.a_bytes + (size_t)bs * L.bstage_bytes + kEpiBytes + kCtrlBytes;
@@ -176,7 +180,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     auto a_at = [&](int s) { return aring + (size_t)s * L.a_bytes; };
     auto bhi_at = [&](int s) { return bring + (size_t)s * L.bstage_bytes; };
-    auto blo_at = [&](int s) { return bhi_at(s) + L.b_bytes; };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < AS; ++s) {
@@ -207,7 +210,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t tmem_base = *tmem_slot;
 
     const int64_t tiles = P.tiles;
-    const int kchunks = P.kchunks;
+    const int kstages = P.kstages;
     const int64_t mper = (P.inner + kBM - 1) / kBM;
 
     if (warp == 0) {
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int i = 0; i < kMaxA; ++i) issued[i] = -1;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 const int64_t mt = t % P.tiles_m;
-                for (int kc = 0; kc < kchunks; ++kc) {
+                for (int st = 0; st < kstages; ++st) {
                     if (!mbar_wait(&a_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     if (P.ldg_a) {
                         // no copy: the stage is free for the converters, which load A themselves
@@ -230,14 +233,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     issued[s] = (int)ph;
                     mbar_expect_tx(&a_full[s], L.a_bytes);
-                    if (GEOM == GEOM_MN && P.fold_kb > 1) {
-                        // folded tile: slices mt*KB .. +KB-1, the map ordered (i, k, l)
-                        tma_load_3d(a_at(s), &amap, &a_full[s], 0, (int)(mt * P.fold_kb), kc * kBK);
-                    } else if (GEOM == GEOM_MN) {
-                        const int64_t k = mt / mper, ib = mt - k * mper;
-                        tma_load_3d(a_at(s), &amap, &a_full[s], (int)(ib * kBM), kc * kBK, (int)k);
-                    } else {
-                        tma_load_2d(a_at(s), &amap, &a_full[s], kc * kBK, (int)(mt * kBM));
+                    // kSub boxes; a box past n_q (odd chunk count) is zero-filled by the copy
+#pragma unroll
+                    for (int sub = 0; sub < kSub; ++sub) {
+                        uint8_t* dst = a_at(s) + sub * L.asub_bytes;
+                        const int l0 = (st * kSub + sub) * kBK;
+                        if (GEOM == GEOM_MN && P.fold_kb > 1) {
+                            // folded tile: slices mt*KB .. +KB-1, the map ordered (i, k, l)
+                            tma_load_3d(dst, &amap, &a_full[s], 0, (int)(mt * P.fold_kb), l0);
+                        } else if (GEOM == GEOM_MN) {
+                            const int64_t k = mt / mper, ib = mt - k * mper;
+                            tma_load_3d(dst, &amap, &a_full[s], (int)(ib * kBM), l0, (int)k);
+                        } else {
+                            tma_load_2d(dst, &amap, &a_full[s], l0, (int)(mt * kBM));
+                        }
                     }
                     if (++s == AS) { s = 0; ph ^= 1; }
                 }
@@ -259,13 +268,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int i = 0; i < kMaxB; ++i) issued[i] = -1;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 const int64_t jb = t / P.tiles_m;
-                for (int kc = 0; kc < kchunks; ++kc) {
+                for (int st = 0; st < kstages; ++st) {
                     if (!mbar_wait(&b_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&b_full[s], 2 * L.b_bytes);
-                    const uint8_t* img = P.bimg + ((size_t)(jb * kchunks + kc) * 2) * L.b_bytes;
-                    bulk_load(bhi_at(s), img, L.b_bytes, &b_full[s]);
-                    bulk_load(blo_at(s), img + L.b_bytes, L.b_bytes, &b_full[s]);
+                    mbar_expect_tx(&b_full[s], L.bstage_bytes);
+                    // the image holds kstages * kSub sub-blocks per j block: one copy per stage
+                    const uint8_t* img = P.bimg + ((size_t)(jb * kstages + st) * L.bstage_bytes);
+                    bulk_load(bhi_at(s), img, L.bstage_bytes, &b_full[s]);
                     if (++s == BS) { s = 0; ph ^= 1; }
                 }
             }
@@ -279,6 +288,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ------------------------------------------------------------- MMA issuer
         if (lane == 0) {
             const uint32_t idesc = idesc_bf16(P.nt, GEOM == GEOM_MN);
+            // descriptors of stage 0's first sub-block; a descriptor's start-address field is
+            // address / 16 in its low bits, so other stages and parts are plain additions
+            const uint64_t da0 = GEOM == GEOM_MN ? smem_desc(su32(aring), 1024u, 2048u, kLayoutSW128)
+                                                 : smem_desc(su32(aring), 16u, 256u, kLayoutSW32);
+            const uint64_t db0 = smem_desc(su32(bring), 16u, 256u, kLayoutSW32);
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             int ab = 0;
@@ -288,26 +302,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (!mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag)) break;
                 tc_fence_after();
                 const uint32_t dcol = tmem_base + (uint32_t)(ab * P.nt);
-                for (int kc = 0; kc < kchunks; ++kc) {
+                for (int st = 0; st < kstages; ++st) {
                     if (!mbar_wait(&b_full[bs], bph, abort_flag) || !mbar_wait(&a_conv[as], aph, abort_flag)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t ahi = su32(a_at(as)), alo = ahi + L.abf_bytes;
-                    uint64_t dahi, dalo;
-                    if (GEOM == GEOM_MN) {
-                        dahi = smem_desc(ahi, 1024u, 2048u, kLayoutSW128);
-                        dalo = smem_desc(alo, 1024u, 2048u, kLayoutSW128);
-                    } else {
-                        dahi = smem_desc(ahi, 16u, 256u, kLayoutSW32);
-                        dalo = smem_desc(alo, 16u, 256u, kLayoutSW32);
+                    const uint64_t da = da0 + ((uint64_t)(as * L.a_bytes) >> 4);
+                    const uint64_t db = db0 + ((uint64_t)(bs * L.bstage_bytes) >> 4);
+#pragma unroll
+                    for (int sub = 0; sub < kSub; ++sub) {
+                        const uint64_t dahi = da + (uint64_t)((sub * L.asub_bytes) >> 4);
+                        const uint64_t dalo = dahi + (uint64_t)(L.abf_bytes >> 4);
+                        const uint64_t dbhi = db + (uint64_t)((sub * 2 * L.b_bytes) >> 4);
+                        const uint64_t dblo = dbhi + (uint64_t)(L.b_bytes >> 4);
+                        mma_bf16(dcol, dahi, dbhi, idesc, (st == 0 && sub == 0) ? 0u : 1u);
+                        mma_bf16(dcol, dahi, dblo, idesc, 1u);
+                        mma_bf16(dcol, dalo, dbhi, idesc, 1u);
                     }
-                    const uint64_t dbhi = smem_desc(su32(bhi_at(bs)), 16u, 256u, kLayoutSW32);
-                    const uint64_t dblo = smem_desc(su32(blo_at(bs)), 16u, 256u, kLayoutSW32);
-                    mma_bf16(dcol, dahi, dbhi, idesc, kc == 0 ? 0u : 1u);
-                    mma_bf16(dcol, dahi, dblo, idesc, 1u);
-                    mma_bf16(dcol, dalo, dbhi, idesc, 1u);
                     mma_commit(&a_empty[as]);   // stages free once these MMAs have read them
                     mma_commit(&b_empty[bs]);
                     if (++as == AS) { as = 0; aph ^= 1; }
@@ -325,83 +337,90 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp < 3 + kConvWarps) {
         // ------------------------------------------------------------- converters (in place)
         // kConvGroups groups of kGroupWarps warps; group g converts the stages with sequence number
-        // n, n % kConvGroups == g, so that many tiles are converted at once.
+        // n, n % kConvGroups == g (their kSub sub-blocks one after the other), so that several
+        // stages are converted at once.
         const int g = (warp - 3) / kGroupWarps;
         const int gt = threadIdx.x - 96 - g * kGroupWarps * 32;   // 0 .. kGroupWarps*32-1
         const bool odd = lane & 1;
         constexpr int kIters = (kBM * kBK / 4) / (kGroupWarps * 32);
         bool ok = true;
-        int64_t n = 0;   // sequence number of the chunk across this CTA's tiles
-        // Every thread of a group runs every iteration of its parity and reaches the group barrier
+        int64_t n = 0;   // sequence number of the stage across this CTA's tiles
+        // Every thread of a group runs every iteration of its residue and reaches the group barrier
         // the same number of times; once the CTA aborts, the waits are skipped and no work is done.
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-            for (int kc = 0; kc < kchunks; ++kc, ++n) {
+            for (int st = 0; st < kstages; ++st, ++n) {
                 if ((int)(n % kConvGroups) != g) continue;
                 const int s = (int)(n % AS);
                 const uint32_t ph = (uint32_t)((n / AS) & 1);
                 const bool got = ok && mbar_wait(&a_full[s], ph, abort_flag);
                 const bool have = __all_sync(0xffffffffu, got);
                 if (!have) ok = false;
-                uint8_t* buf = a_at(s);
-                float4 x[kIters];
-                uint32_t off[kIters];
-                // tile origin for the converters' own loads of A (ldg_a): slice k / first row
-                const int64_t mt = t % P.tiles_m;
-                const int64_t tk = GEOM == GEOM_MN ? mt / mper : 0;
-                const int64_t r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
-#pragma unroll
-                for (int it = 0; it < kIters; ++it) {
-                    const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
-                    if (GEOM == GEOM_MN) {
-                        const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
-                        if (have && P.ldg_a) {
-                            // elements (l, i .. i+3) of slice tk (of slice tk * KB + row / IB when
-                            // folded), zero outside A
-                            const int64_t gl = (int64_t)kc * kBK + l;
-                            const int64_t sk = P.fold_kb > 1 ? mt * P.fold_kb + ((w * 4) >> P.fold_ib_shift) : tk;
-                            const int64_t i = P.fold_kb > 1 ? ((w * 4) & ((1 << P.fold_ib_shift) - 1)) : r0 + w * 4;
-                            const float* src = P.a + (sk * P.nq + gl) * P.inner + i;
-                            const bool lv = gl < P.nq && sk < P.outer;
-                            x[it].x = (lv && i < P.inner) ? __ldg(src) : 0.0f;
-                            x[it].y = (lv && i + 1 < P.inner) ? __ldg(src + 1) : 0.0f;
-                            x[it].z = (lv && i + 2 < P.inner) ? __ldg(src + 2) : 0.0f;
-                            x[it].w = (lv && i + 3 < P.inner) ? __ldg(src + 3) : 0.0f;
-                        } else if (have) {
-                            x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
-                        }
-                        off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
-                    } else {
-                        const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
-                        if (have && P.ldg_a) {
-                            // elements (row, l .. l+3) of the contiguous fibre row, zero outside A
-                            const int64_t row = r0 + k, gl = (int64_t)kc * kBK + lc * 4;
-                            const float* src = P.a + row * P.nq + gl;
-                            const bool rv = row < P.outer;
-                            x[it].x = (rv && gl < P.nq) ? __ldg(src) : 0.0f;
-                            x[it].y = (rv && gl + 1 < P.nq) ? __ldg(src + 1) : 0.0f;
-                            x[it].z = (rv && gl + 2 < P.nq) ? __ldg(src + 2) : 0.0f;
-                            x[it].w = (rv && gl + 3 < P.nq) ? __ldg(src + 3) : 0.0f;
-                        } else if (have) {
-                            x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
-                        }
-                        off[it] = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
-                    }
-                }
-                conv_barrier(g);   // the whole FP32 tile is in registers before it is overwritten
-                if (have) {
+#pragma unroll 1
+                for (int sub = 0; sub < kSub; ++sub) {
+                    const int kc = st * kSub + sub;
+                    uint8_t* buf = a_at(s) + sub * L.asub_bytes;
+                    float4 x[kIters];
+                    uint32_t off[kIters];
+                    // tile origin for the converters' own loads of A (ldg_a): slice k / first row
+                    const int64_t mt = t % P.tiles_m;
+                    const int64_t tk = GEOM == GEOM_MN ? mt / mper : 0;
+                    const int64_t r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
 #pragma unroll
                     for (int it = 0; it < kIters; ++it) {
-                        uint32_t h0, l0, h1, l1;
-                        split2(x[it].x, x[it].y, h0, l0);
-                        split2(x[it].z, x[it].w, h1, l1);
-                        // Lane pairs hold 8 consecutive elements: the even lane assembles the hi
-                        // chunk, the odd lane the lo chunk.
-                        const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
-                        const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
-                        const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
-                        if (!odd) *reinterpret_cast<uint4*>(buf + off[it]) = pack4(h0, h1, got0, got1);
-                        else *reinterpret_cast<uint4*>(buf + L.abf_bytes + off[it]) = pack4(got0, got1, l0, l1);
+                        const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
+                        if (GEOM == GEOM_MN) {
+                            const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
+                            if (have && P.ldg_a) {
+                                // elements (l, i .. i+3) of slice tk (of slice tk * KB + row / IB when
+                                // folded), zero outside A
+                                const int64_t gl = (int64_t)kc * kBK + l;
+                                const int64_t sk = P.fold_kb > 1 ? mt * P.fold_kb + ((w * 4) >> P.fold_ib_shift) : tk;
+                                const int64_t i = P.fold_kb > 1 ? ((w * 4) & ((1 << P.fold_ib_shift) - 1)) : r0 + w * 4;
+                                const float* src = P.a + (sk * P.nq + gl) * P.inner + i;
+                                const bool lv = gl < P.nq && sk < P.outer;
+                                x[it].x = (lv && i < P.inner) ? __ldg(src) : 0.0f;
+                                x[it].y = (lv && i + 1 < P.inner) ? __ldg(src + 1) : 0.0f;
+                                x[it].z = (lv && i + 2 < P.inner) ? __ldg(src + 2) : 0.0f;
+                                x[it].w = (lv && i + 3 < P.inner) ? __ldg(src + 3) : 0.0f;
+                            } else if (have) {
+                                x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
+                            }
+                            off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
+                        } else {
+                            const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
+                            if (have && P.ldg_a) {
+                                // elements (row, l .. l+3) of the contiguous fibre row, zero outside A
+                                const int64_t row = r0 + k, gl = (int64_t)kc * kBK + lc * 4;
+                                const float* src = P.a + row * P.nq + gl;
+                                const bool rv = row < P.outer;
+                                x[it].x = (rv && gl < P.nq) ? __ldg(src) : 0.0f;
+                                x[it].y = (rv && gl + 1 < P.nq) ? __ldg(src + 1) : 0.0f;
+                                x[it].z = (rv && gl + 2 < P.nq) ? __ldg(src + 2) : 0.0f;
+                                x[it].w = (rv && gl + 3 < P.nq) ? __ldg(src + 3) : 0.0f;
+                            } else if (have) {
+                                x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                            }
+                            off[it] = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
+                        }
                     }
+                    conv_barrier(g);   // the whole FP32 tile is in registers before it is overwritten
+                    if (have) {
+#pragma unroll
+                        for (int it = 0; it < kIters; ++it) {
+                            uint32_t h0, l0, h1, l1;
+                            split2(x[it].x, x[it].y, h0, l0);
+                            split2(x[it].z, x[it].w, h1, l1);
+                            // Lane pairs hold 8 consecutive elements: the even lane assembles the hi
+                            // chunk, the odd lane the lo chunk.
+                            const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
+                            const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
+                            const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
+                            if (!odd) *reinterpret_cast<uint4*>(buf + off[it]) = pack4(h0, h1, got0, got1);
+                            else *reinterpret_cast<uint4*>(buf + L.abf_bytes + off[it]) = pack4(got0, got1, l0, l1);
+                        }
+                    }
+                }
+                if (have) {
                     fence_proxy_async();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&a_conv[s]);
@@ -761,8 +780,9 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                     const V* box = reinterpret_cast<const V*>(ring + s * SB) + tid;
                     const T* brow = bs + (size_t)(kc - kc0) * P.lb * MB;
                     const int lb = P.lb;
-                    // all LB reads up front, except at MB = 16 where the registers go to acc
-                    constexpr int PRE = MB < 16 ? LB : 1;
+                    // all LB reads up front, except at MB = 16 with two CTAs per SM, where the
+                    // registers go to acc
+                    constexpr int PRE = (MB < 16 || CPS == 1) ? LB : 1;
                     V av[PRE];
 #pragma unroll
                     for (int l = 0; l < PRE; ++l) av[l] = box[l * (NP / W)];   // in the stage even past lb
@@ -1055,6 +1075,7 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
     const int jblocks = (int)((v.m + nt - 1) / nt);
     const int kchunks = (int)((v.nq + kBK - 1) / kBK);
+    const int kstages = (kchunks + kSub - 1) / kSub;
     CUtensorMap amap, cmap;
     TcParams P{};
     P.ldg_a = tma_a_ok(v, geom) ? 0 : 1;
@@ -1086,13 +1107,15 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     P.nt = nt;
     P.jblocks = jblocks;
     P.kchunks = kchunks;
+    P.kstages = kstages;
     size_t smem = 0;
     if (!choose_stages(nt, P.fstages, P.ostages, smem)) return cudaErrorNotSupported;
 
-    const int64_t total = (int64_t)jblocks * kchunks * nt * 2;
+    // the image holds kstages * kSub sub-blocks per j block (zero past n_q)
+    const int64_t total = (int64_t)jblocks * (kstages * kSub) * nt * 2;
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-    split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks, kchunks,
-                                          img);
+    split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks,
+                                          kstages * kSub, img);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const int grid = (int)std::min<int64_t>(P.tiles, sms);
@@ -1527,8 +1550,8 @@ size_t tc_image_bytes(const View3& v)
 {
     const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
     const int64_t jblocks = (v.m + nt - 1) / nt;
-    const int64_t kchunks = (v.nq + kBK - 1) / kBK;
-    return (size_t)(jblocks * kchunks * 2) * smem_layout(nt).b_bytes;
+    const int64_t kpad = (v.nq + kSub * kBK - 1) / (kSub * kBK) * kSub;   // sub-blocks, a whole number of stages
+    return (size_t)(jblocks * kpad * 2) * smem_layout(nt).b_bytes;
 }
 
 cudaError_t launch_tc_noalloc(const View3& v, cudaStream_t s, int* kid)
