@@ -14,12 +14,12 @@
 // MMA shape M = 128, N = NT (<= 256, the rows of B in this tile), K = 16 per
 // instruction, 32 l (two sub-blocks of 16, six MMAs) per pipeline stage.
 //
-// Warp roles (480 threads, one CTA per SM, persistent over tiles):
+// Warp roles (736 threads, one CTA per SM, persistent over tiles):
 //   warp 0     TMA producer of the FP32 A tile (tensor map).
 //   warp 1     TMEM allocator and MMA issuer (one elected lane).
 //   warp 2     bulk copies of the pre-split B_hi/B_lo image of this stage.
-//   warps 3-10 converters: FP32 tile -> bf16 hi/lo in the swizzled UMMA layout.
-//   warps 11-14 epilogue: TMEM -> registers -> global C (double-buffered accumulator).
+//   warps 3-18 converters: FP32 tile -> bf16 hi/lo in the swizzled UMMA layout.
+//   warps 19-22 epilogue: TMEM -> registers -> global C (double-buffered accumulator).
 // Every mbarrier wait is bounded (4 s of %globaltimer); on expiry the CTA raises
 // an abort flag, records an error in the device status word, drains its own
 // bulk copies, frees TMEM and returns.
@@ -40,7 +40,7 @@
 namespace tlibttm {
 namespace {
 
-constexpr int kConvWarps = 8;                   // converter warps
+constexpr int kConvWarps = 16;                  // converter warps
 constexpr int kConvGroups = 4;                  // groups converting different stages at the same time
 constexpr int kGroupWarps = kConvWarps / kConvGroups;
 constexpr int kThreads = (3 + kConvWarps + 4) * 32;  // A producer, MMA, B producer, converters, 4 epilogue warps
@@ -137,9 +137,11 @@ __host__ inline bool choose_stages(int nt, int& as, int& bs, size_t& smem)
 {
     const SmemLayout L = smem_layout(nt);
     const size_t avail = kSmemBudget - 1024 - kCtrlBytes - kEpiBytes;
+    // at least kConvGroups A stages: each converter group waits on its own stage's barrier by
+    // phase parity, which stays unambiguous only while the groups cover at most one ring pass
     bs = kMaxB;
-    while (bs > 2 && (size_t)bs * L.bstage_bytes + 4 * L.a_bytes > avail) --bs;
-    if ((size_t)bs * L.bstage_bytes + 4 * L.a_bytes > avail) return false;
+    while (bs > 2 && (size_t)bs * L.bstage_bytes + kConvGroups * L.a_bytes > avail) --bs;
+    if ((size_t)bs * L.bstage_bytes + kConvGroups * L.a_bytes > avail) return false;
     as = (int)((avail - (size_t)bs * L.bstage_bytes) / L.a_bytes);
     if (as > kMaxA) as = kMaxA;
     smem = 1024 + (size_t)as * L.a_bytes + (size_t)bs * L.bstage_bytes + kEpiBytes + kCtrlBytes;
