@@ -524,11 +524,15 @@ __global__ void __launch_bounds__(256) rowdot_kernel(View3 v)
 // rowflat: small m, contiguous fibres of at most kFlatMaxNq elements (inner == 1, short rows).
 // A warp's wr consecutive rows are wr * nq contiguous elements: the warp copies them with
 // coalesced loads into shared memory with rows padded to nq + 1 (conflict-free row reads), then
-// each lane computes every 32nd row. B sits in shared memory as bs[l][j].
+// each lane computes every 32nd row. B sits in shared memory as bs[l][j]. With STAGE, the m
+// outputs of 32 consecutive rows (32 * m contiguous elements of C) are staged in shared memory
+// (rows padded to an odd stride) and written with coalesced stores, 32 consecutive elements per
+// instruction; without it each lane stores its own row (a stride of m elements between lanes),
+// which measured faster where a row's outputs are short or the fibres long.
 // ---------------------------------------------------------------------------------------------
 constexpr int kFlatMaxNq = 16;
 
-template <typename T, int MB>
+template <typename T, int MB, bool STAGE>
 __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
 {
     constexpr int MBP = MB < 4 ? 4 : MB;
@@ -538,6 +542,8 @@ __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     T* tile = smf + (size_t)warp * wr * stride;
     T* bs = smf + (size_t)8 * wr * stride;
+    const int ms = (int)v.m | 1;                                   // odd row stride of the staged outputs
+    T* ostage = bs + (size_t)nq * MBP + (size_t)warp * 32 * ms;
     const T* __restrict__ B = static_cast<const T*>(v.b);
     for (int e = threadIdx.x; e < nq * MBP; e += blockDim.x) {
         const int l = e / MBP, j = e - l * MBP;
@@ -558,20 +564,52 @@ __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
     }
     __syncwarp();
     T* __restrict__ Cp = static_cast<T*>(v.c);
-    for (int r = lane; r < nrow; r += 32) {
-        T acc[MB];
+    const int m = (int)v.m;
+    // e / m == umulhi(e, ceil(2^32 / m)) for e < 32 * m (m > 1)
+    const uint32_t minv = m > 1 ? (uint32_t)((0x100000000ull + m - 1) / m) : 0u;
+    if constexpr (!STAGE) {
+        for (int r = lane; r < nrow; r += 32) {
+            T acc[MB];
 #pragma unroll
-        for (int j = 0; j < MB; ++j) acc[j] = T(0);
-        const T* row = tile + r * stride;
-        for (int l = 0; l < nq; ++l) {
-            const T a = row[l];
+            for (int j = 0; j < MB; ++j) acc[j] = T(0);
+            const T* row = tile + r * stride;
+            for (int l = 0; l < nq; ++l) {
+                const T a = row[l];
 #pragma unroll
-            for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bs[l * MBP + j], acc[j]);
+                for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bs[l * MBP + j], acc[j]);
+            }
+            T* cp = Cp + (wrow0 + r) * (int64_t)m;
+#pragma unroll
+            for (int j = 0; j < MB; ++j)
+                if (j < m) cp[j] = acc[j];
         }
-        T* cp = Cp + (wrow0 + r) * v.m;
+        return;
+    }
+    for (int r0 = 0; r0 < nrow; r0 += 32) {
+        const int r = r0 + lane;
+        if (r < nrow) {
+            T acc[MB];
 #pragma unroll
-        for (int j = 0; j < MB; ++j)
-            if (j < v.m) cp[j] = acc[j];
+            for (int j = 0; j < MB; ++j) acc[j] = T(0);
+            const T* row = tile + r * stride;
+            for (int l = 0; l < nq; ++l) {
+                const T a = row[l];
+#pragma unroll
+                for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bs[l * MBP + j], acc[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < MB; ++j)
+                if (j < m) ostage[lane * ms + j] = acc[j];
+        }
+        __syncwarp();
+        // rows r0 .. r0 + nr - 1: nr * m contiguous outputs from C[(wrow0 + r0) * m]
+        const int nr = (nrow - r0) < 32 ? (nrow - r0) : 32;
+        T* cp = Cp + (wrow0 + r0) * (int64_t)m;
+        for (int e = lane; e < nr * m; e += 32) {
+            const int rr = m > 1 ? (int)__umulhi((uint32_t)e, minv) : e;
+            cp[e] = ostage[rr * ms + (e - rr * m)];
+        }
+        __syncwarp();
     }
 }
 
@@ -828,18 +866,36 @@ cudaError_t rowdot_dispatch_v(const View3& v, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <typename T, int MB, bool STAGE>
+cudaError_t rowflat_launch_s(const View3& v, cudaStream_t s)
+{
+    // rows per warp: about 4 KB of A, a multiple of 32, with the block's tiles, B and the output
+    // staging (8 warps x 32 rows x (m | 1)) within 44 KB of shared memory where that allows 32 rows
+    const int64_t es = (int64_t)sizeof(T), ms = STAGE ? (v.m | 1) : 0;
+    const int64_t fixed = 16 * 16 * es + 8 * 32 * ms * es;
+    const int64_t want = 4096 / (v.nq * es);
+    const int64_t cap = (44 * 1024 - fixed) / (8 * (v.nq + 1) * es);
+    const int wr = (int)std::max<int64_t>(32, std::min(want, cap) / 32 * 32);
+    const size_t smem = ((size_t)8 * wr * (v.nq + 1) + (size_t)v.nq * (MB < 4 ? 4 : MB) + (size_t)8 * 32 * ms) * sizeof(T);
+    const int64_t blocks = ceil_div(v.outer, (int64_t)8 * wr);
+    if (smem > 48 * 1024) {
+        // staged double outputs of m up to 16 with 32-row tiles: up to 70 KB
+        const cudaError_t e = cudaFuncSetAttribute(rowflat_kernel<T, MB, STAGE>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    rowflat_kernel<T, MB, STAGE><<<(unsigned)blocks, 256, smem, s>>>(v, wr);
+    return cudaGetLastError();
+}
+
+// Staged (coalesced) output stores where a row's outputs take at least 64 bytes, or at least 32
+// bytes with fibres of at most 4 elements (measured on A of 2^26 elements, n_q 2..16, m 4..16).
 template <typename T, int MB>
 cudaError_t rowflat_launch(const View3& v, cudaStream_t s)
 {
-    // rows per warp: about 4 KB of A, a multiple of 32, with the block's tiles within 44 KB of
-    // shared memory (no opt-in needed)
-    const int64_t want = 4096 / (v.nq * (int64_t)sizeof(T));
-    const int64_t cap = (44 * 1024 - 16 * 16 * (int64_t)sizeof(T)) / (8 * (v.nq + 1) * (int64_t)sizeof(T));
-    const int wr = (int)std::max<int64_t>(32, std::min(want, cap) / 32 * 32);
-    const size_t smem = ((size_t)8 * wr * (v.nq + 1) + (size_t)v.nq * (MB < 4 ? 4 : MB)) * sizeof(T);
-    const int64_t blocks = ceil_div(v.outer, (int64_t)8 * wr);
-    rowflat_kernel<T, MB><<<(unsigned)blocks, 256, smem, s>>>(v, wr);
-    return cudaGetLastError();
+    const int64_t ob = v.m * (int64_t)sizeof(T);
+    const bool stage = ob >= 64 || (ob >= 32 && v.nq <= 4);
+    return stage ? rowflat_launch_s<T, MB, true>(v, s) : rowflat_launch_s<T, MB, false>(v, s);
 }
 
 template <typename T, int NQ>
