@@ -782,18 +782,15 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                     const V* box = reinterpret_cast<const V*>(ring + s * SB) + tid;
                     const T* brow = bs + (size_t)(kc - kc0) * P.lb * MB;
                     const int lb = P.lb;
-                    // all LB reads up front, except at MB = 16 with two CTAs per SM, where the
-                    // registers go to acc
-                    constexpr int PRE = (MB < 16 || CPS == 1) ? LB : 1;
-                    V av[PRE];
+                    // all LB reads up front (the builds for m = 16 run one CTA per SM and have
+                    // the registers)
+                    V av[LB];
 #pragma unroll
-                    for (int l = 0; l < PRE; ++l) av[l] = box[l * (NP / W)];   // in the stage even past lb
+                    for (int l = 0; l < LB; ++l) av[l] = box[l * (NP / W)];   // in the stage even past lb
 #pragma unroll
                     for (int l = 0; l < LB; ++l) {
                         if (l >= lb) break;
-                        V a1;
-                        if constexpr (PRE == 1) a1 = l == 0 ? av[0] : box[l * (NP / W)];
-                        else a1 = av[l];
+                        const V a1 = av[l];
                         const T* a = reinterpret_cast<const T*>(&a1);
                         const T* bl = brow + l * MB;
                         if constexpr (MB % W == 0) {
