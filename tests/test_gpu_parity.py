@@ -167,6 +167,37 @@ def test_stream_cols_box_shapes(cuda, oracle_c, dtype):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_stream_cols_two_ctas_per_sm(cuda, oracle_c, dtype):
+    """Column mode with at least as many tiles as SMs and m <= 8 runs the 96-register build two
+    CTAs per SM with 48 KB rings; cover it with one unit per tile and with the l range split three
+    (float) or two (double) ways (128 x 1280 slices, n_q 256, m 2), several units per CTA, and the
+    m buckets 1, 4 and 8."""
+    import torch
+    from ttm_b200.selector import lib
+    rng = np.random.default_rng(22)
+    shapes = [(256, 1024, 8, 8), (64, 4096, 20, 3), (128, 1280, 256, 2), (512, 384, 40, 8), (256, 640, 64, 1)]
+    dt = _lib.F32 if dtype == np.float32 else _lib.F64
+    for n, (inner, outer, nq, m) in enumerate(shapes):
+        na = [inner, nq, outer]
+        nc = [inner, m, outer]
+        pia = [1, 2, 3]
+        md = dict(na=na, wa=ka.dense_strides(na, pia), pia=pia, nb=[m, nq], pib=[1, 2] if n % 2 else [2, 1],
+                  nc=nc, wc=ka.dense_strides(nc, pia))
+        a = rng.standard_normal(int(np.prod(na))).astype(dtype)
+        b = rng.standard_normal(m * nq).astype(dtype)
+        ta, tb = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+        tc = torch.full((int(np.prod(nc)),), float("nan"), dtype=ta.dtype, device=cuda)
+        rc = lib().tlibttm_ttm_sched(dt, 6, 2, 3, ta.data_ptr(), _lib.sz(na), _lib.sz(md["wa"]), _lib.sz(pia),
+                                     tb.data_ptr(), _lib.sz(md["nb"]), _lib.sz(md["pib"]), tc.data_ptr(), _lib.sz(nc),
+                                     _lib.sz(md["wc"]), None)
+        assert rc == 0 and _lib.last_kernel() == "stream_cols", (inner, outer, nq, m, rc)
+        c = tc.cpu().numpy()
+        ref = np.zeros(int(np.prod(nc)), dtype=dtype)
+        oracle_c.ttm(2, a, na, md["wa"], pia, b, md["nb"], md["pib"], ref, nc, md["wc"])
+        assert relerr(c, ref) <= (1e-14 if dtype == np.float64 else 2e-6), (inner, outer, nq, m)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_stream_rows_contiguous_fibres(cuda, oracle_c, dtype):
     """The TMA-fed small-m kernel in row mode (q = pi_1, contiguous fibres) through schedule 6:
     partial l chunks, row counts off the 512-row tile (second box partly or wholly past the end), few tiles (l split with partial tiles added
