@@ -60,7 +60,6 @@ __device__ __forceinline__ void store_vec(T* p, const T (&r)[W])
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
 
-
 // ---------------------------------------------------------------------------------------------
 // simt_gemm
 //   AK   : A is K-major (inner == 1, fibres contiguous); otherwise rows (i) are contiguous.
@@ -542,8 +541,6 @@ __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     T* tile = smf + (size_t)warp * wr * stride;
     T* bs = smf + (size_t)8 * wr * stride;
-    const int ms = (int)v.m | 1;                                   // odd row stride of the staged outputs
-    T* ostage = bs + (size_t)nq * MBP + (size_t)warp * 32 * ms;
     const T* __restrict__ B = static_cast<const T*>(v.b);
     for (int e = threadIdx.x; e < nq * MBP; e += blockDim.x) {
         const int l = e / MBP, j = e - l * MBP;
@@ -565,8 +562,6 @@ __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
     __syncwarp();
     T* __restrict__ Cp = static_cast<T*>(v.c);
     const int m = (int)v.m;
-    // e / m == umulhi(e, ceil(2^32 / m)) for e < 32 * m (m > 1)
-    const uint32_t minv = m > 1 ? (uint32_t)((0x100000000ull + m - 1) / m) : 0u;
     if constexpr (!STAGE) {
         for (int r = lane; r < nrow; r += 32) {
             T acc[MB];
@@ -585,6 +580,11 @@ __global__ void __launch_bounds__(256) rowflat_kernel(View3 v, int wr)
         }
         return;
     }
+    // staged: this warp's 32 x (m | 1) outputs after B (odd row stride, conflict-free writes)
+    const int ms = m | 1;
+    T* ostage = bs + (size_t)nq * MBP + (size_t)warp * 32 * ms;
+    // e / m == umulhi(e, ceil(2^32 / m)) for e < 32 * m (m > 1)
+    const uint32_t minv = m > 1 ? (uint32_t)((0x100000000ull + m - 1) / m) : 0u;
     for (int r0 = 0; r0 < nrow; r0 += 32) {
         const int r = r0 + lane;
         if (r < nrow) {
