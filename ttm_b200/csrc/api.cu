@@ -517,9 +517,6 @@ int run(const Args& x, int precision, void* stream)
 }
 
 // ---- plans ----------------------------------------------------------------------------------
-// Under precision auto, a batched problem takes the tensor-core path only from this many
-// elements of A on; smaller ones run inside the grouped launch.
-constexpr int64_t kAutoTcMinElems = int64_t(1) << 22;
 // Batched plans: problems with at least this many elements of A take their own launch of the
 // kernel the planner picks for them (bf16x3 under auto/bf16x3 for m > 16, the small-m kernels
 // for m <= 16); smaller ones share the grouped launch. Measured on the 512-problem workload, the

@@ -44,7 +44,6 @@ constexpr int kConvWarps = 16;                  // converter warps
 constexpr int kConvGroups = 4;                  // groups converting different stages at the same time
 constexpr int kGroupWarps = kConvWarps / kConvGroups;
 constexpr int kThreads = (3 + kConvWarps + 4) * 32;  // A producer, MMA, B producer, converters, 4 epilogue warps
-constexpr int kConvThreads = kConvWarps * 32;
 constexpr int kBM = 128;       // MMA M
 constexpr int kBK = 16;        // l per sub-block (one MMA K step)
 constexpr int kSub = 2;        // sub-blocks per pipeline stage: 3 * kSub MMAs per barrier round
