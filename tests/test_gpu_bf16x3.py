@@ -1,7 +1,7 @@
 """bf16x3 tensor-core path (tcgen05): FP32-accurate results from BF16 products.
 
 Bar: relative Frobenius error <= 1e-5 against the FP64-accumulated oracle on
-N(0,1) data (the north-star tolerance for the split-BF16 path), over both
+N(0,1) data (the required accuracy of the split-BF16 path), over both
 tile geometries (i-contiguous slices and q = pi_1), partial tiles in every
 dimension, m above and below one MMA N tile, and both B layouts.
 """

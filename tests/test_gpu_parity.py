@@ -2,7 +2,7 @@
 
 Tolerances: plain FP64 within 1e-13 and plain FP32 within 2e-6 relative
 Frobenius error of each case against the reference's own outputs / the oracle
-(the north-star bar for plain FP32 is 1e-5); exact-integer known answers
+(the required bound for plain FP32 is 1e-5); exact-integer known answers
 within 4 ULP as in the reference's unit test.
 """
 import os

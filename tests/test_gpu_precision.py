@@ -1,6 +1,6 @@
 """The 8-bit tensor-core paths through the C ABI on a CUDA device.
 
-ozaki (double): within 1e-12 relative Frobenius error of the FP64 oracle,
+ozaki (double): within 1e-12 relative Frobenius error of the FP64 oracle (the required bound),
 on N(0,1) data and on magnitudes log-uniform over [1e-4, 1e4]; exact on small integers.
 fp8 (float): within 1e-4 of the same product with the operands rounded as the path rounds them
 (tests/emulation.py), so the check is on the kernels, not on e4m3's own error; that error is
