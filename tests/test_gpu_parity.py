@@ -305,7 +305,7 @@ def test_kernel_selection_and_strided(cuda):
     assert np.all(c[mask] == 7.5)
 
 
-def test_cfg1_full_size(cuda, oracle_c):
+def test_a256_cube_q2_m128_full_size(cuda, oracle_c):
     """A 256^3 first-order, q=2, B (128, 256) column-major, U[-1,1] from seed 0 (the reference's CPU case)."""
     rng = np.random.default_rng(0)
     na, pia, q, m = [256, 256, 256], [1, 2, 3], 2, 128
