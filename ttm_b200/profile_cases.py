@@ -1,4 +1,4 @@
-"""One TTM case through the C ABI, repeated: the driver the committed ncu summaries are made with.
+"""One TTM case through the C ABI, repeated: the case runner used for ncu captures.
 
     python -m ttm_b200.profile_cases --dtype f32 --precision bf16x3 --na 256,256,256,16 --q 2 \
         --m 256 [--pia 1,2,3,4] [--iters 3]
