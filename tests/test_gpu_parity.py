@@ -240,9 +240,11 @@ def test_short_contiguous_fibres(cuda, oracle_c, dtype):
     rng = np.random.default_rng(31)
     # n_q in {1, 2, 4, 8, 16}: the span kernel (tail spans, m below its bucket, vector and scalar
     # stores); other lengths: the flat-tile kernel
+    # (12, 20001, 16) and (16, 3001, 9): staged outputs whose double build needs more than 48 KB of
+    # shared memory (the launch opts in)
     for n, (nq, outer, m) in enumerate(((1, 5000, 1), (2, 70001, 8), (3, 4099, 3), (5, 12345, 16), (16, 33333, 2),
                                         (16, 31, 5), (7, 100000, 1), (4, 9999, 4), (8, 777, 16), (4, 100003, 1),
-                                        (8, 5001, 3), (1, 333, 16))):
+                                        (8, 5001, 3), (1, 333, 16), (12, 20001, 16), (16, 3001, 9))):
         na = [nq, outer]
         pia = [1, 2]
         nc = [m, outer]
