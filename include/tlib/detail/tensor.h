@@ -103,50 +103,69 @@ private:
 
 } // namespace tlib::ttm
 
-// MATLAB-style printing, same format as the reference (tensor.h:131-189):
-// order 1 as a row, order 2 as rows of mode 1, higher orders as nested cat(r, ...).
+// MATLAB-style printing. The text is part of the interface (callers' output is compared
+// against the reference's), so it follows this format exactly; `v` is an element printed with
+// the stream's own formatting, elements taken in memory order of the named modes:
+//   order 1:  "[ \n"   then "v, " for each i1   then "];\n"
+//   order 2:  "[ ... \n"  then per i2: "v, " for each i1, then "...\n"  then "];\n"
+//   order p >= 3: nested blocks. Level r >= 3 opens with "cat(r,...\n", holds one level-(r-1)
+//     block per index of mode r, and closes with ");\n" when r == p, else "), ...\n". The
+//     innermost level-2 block is "[ ... \n", then per i1 the elements over i2 joined by ", " and
+//     ended by "; ...\n", then "],...\n".
+namespace tlib::ttm::detail
+{
 template <class value_type>
-void stream_out(std::ostream& out, tlib::ttm::tensor<value_type> const& a, std::size_t j, unsigned r)
+void print_level2(std::ostream& out, tlib::ttm::tensor<value_type> const& a, std::size_t base)
 {
     const auto w = a.strides();
     const auto& n = a.shape();
-    const auto p = a.order();
-    if (r >= 3) {
-        out << "cat(" << r << ",..." << std::endl;
-        for (std::size_t ir = 0; ir < n[r - 1]; ++ir, j += w[r - 1]) stream_out(out, a, j, r - 1);
-        out << (r == p ? ");" : "), ...") << std::endl;
-    } else if (r == 2) {
-        out << "[ ... " << std::endl;
-        for (std::size_t i1 = 0; i1 < n[0]; ++i1, j += w[0]) {
-            std::size_t j2 = 0;
-            for (std::size_t i2 = 0; i2 + 1 < n[1]; ++i2, j2 += w[1]) out << a[j + j2] << ", ";
-            out << a[j + j2] << "; ..." << std::endl;
-        }
-        out << "],..." << std::endl;
+    out << "[ ... " << std::endl;
+    for (std::size_t r = 0; r < n[0]; ++r) {
+        const std::size_t row = base + r * w[0];
+        for (std::size_t c = 0; c < n[1]; ++c) out << a[row + c * w[1]] << (c + 1 < n[1] ? ", " : "; ...");
+        out << std::endl;
     }
+    out << "],..." << std::endl;
 }
+} // namespace tlib::ttm::detail
 
 template <class value_type>
 std::ostream& operator<<(std::ostream& out, tlib::ttm::tensor<value_type> const& a)
 {
     const auto w = a.strides();
     const auto& n = a.shape();
-    const auto p = a.order();
-    std::size_t j = 0;
+    const std::size_t p = a.order();
     if (p == 1u) {
         out << "[ " << std::endl;
-        for (std::size_t i1 = 0; i1 < n[0]; ++i1, j += w[0]) out << a[j] << ", ";
+        for (std::size_t i = 0; i < n[0]; ++i) out << a[i * w[0]] << ", ";
         out << "];" << std::endl;
-    } else if (p == 2u) {
+        return out;
+    }
+    if (p == 2u) {
         out << "[ ... " << std::endl;
-        for (std::size_t i2 = 0; i2 < n[1]; ++i2, j += w[1]) {
-            std::size_t j2 = 0;
-            for (std::size_t i1 = 0; i1 < n[0]; ++i1, j2 += w[0]) out << a[j + j2] << ", ";
+        for (std::size_t c = 0; c < n[1]; ++c) {
+            for (std::size_t r = 0; r < n[0]; ++r) out << a[c * w[1] + r * w[0]] << ", ";
             out << "..." << std::endl;
         }
         out << "];" << std::endl;
-    } else {
-        stream_out(out, a, j, static_cast<unsigned>(p));
+        return out;
+    }
+    // p >= 3: walk modes 3..p as an odometer (mode 3 fastest), opening and closing the
+    // cat(...) levels as their indices start and wrap.
+    std::vector<std::size_t> idx(p + 1, 0);
+    for (std::size_t r = p; r >= 3; --r) out << "cat(" << r << ",..." << std::endl;
+    while (true) {
+        std::size_t base = 0;
+        for (std::size_t r = 3; r <= p; ++r) base += idx[r] * w[r - 1];
+        tlib::ttm::detail::print_level2(out, a, base);
+        std::size_t r = 3;
+        for (; r <= p; ++r) {
+            if (++idx[r] < n[r - 1]) break;
+            idx[r] = 0;
+            out << (r == p ? ");" : "), ...") << std::endl;
+        }
+        if (r > p) break;
+        for (std::size_t s = r - 1; s >= 3; --s) out << "cat(" << s << ",..." << std::endl;
     }
     return out;
 }

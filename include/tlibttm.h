@@ -116,9 +116,9 @@ int tlibttm_ttm_ex(int dtype, int precision, unsigned q, unsigned p,
  *
  * Limits: a, b and c must all be device memory of the current device (no host
  * staging); A and C dense under their layout; m > 16 and either inner >= 17
- * or q == pia[0]; and the B image,
- * ceil(m/16)*16 * ceil(n_q/32)*32 * 4 bytes, at most 1 MiB (for example
- * m = 256 with n_q <= 1024). Larger or unsupported problems are rejected with
+ * or q == pia[0]; and the B image, cols(m) * ceil(n_q/32)*32 * 4 bytes with
+ * cols(m) = ceil(m/16)*16 for m <= 256 and ceil(m/256)*256 above, at most
+ * 1 MiB (for example m = 256 with n_q <= 1024, or m = 272 with n_q <= 512). Larger or unsupported problems are rejected with
  * TLIBTTM_ERR_ARG / TLIBTTM_ERR_UNSUPPORTED and a message; nothing is launched.
  *
  * The work is enqueued on `stream`; tlibttm_synchronize reports a failed
@@ -240,6 +240,27 @@ int tlibttm_plan_launches(const tlibttm_plan* plan);
 
 /* Frees the plan, its device buffers and its graph. */
 int tlibttm_plan_destroy(tlibttm_plan* plan);
+
+/*
+ * Host-side fault injection for failure-detection tests (no counterpart in the reference; no
+ * GPU fault is ever raised). Each call sets one injection; TLIBTTM_INJECT_NONE clears them all.
+ *  FAIL_ALLOC       arg = n > 0: the n-th next device allocation of the library fails with
+ *                   cudaErrorMemoryAllocation, and the call that made it returns TLIBTTM_ERR_ALLOC
+ *                   (0 disarms).
+ *  WAIT_NS          arg = bound in ns of the mbarrier waits of later bf16x3 launches (0: the
+ *                   default of 4 s). On expiry the kernel's blocks stop, drain their own copies,
+ *                   free tensor memory and raise the status word that tlibttm_synchronize (and
+ *                   every blocking call) reports as TLIBTTM_ERR_DEVICE.
+ *  SKIP_B_STAGE     arg != 0: the next bf16x3 launch never fills its first B stage, so that its
+ *                   MMA issuer's bounded wait runs out (use with a short WAIT_NS).
+ */
+enum tlibttm_injection {
+    TLIBTTM_INJECT_NONE = 0,
+    TLIBTTM_INJECT_FAIL_ALLOC = 1,
+    TLIBTTM_INJECT_WAIT_NS = 2,
+    TLIBTTM_INJECT_SKIP_B_STAGE = 3
+};
+int tlibttm_inject(int what, long long arg);
 
 /* Text of the last error reported on the calling thread ("" if none). */
 const char* tlibttm_last_error(void);

@@ -40,10 +40,18 @@ REF_POLICIES = [
 ]
 
 
-def build(ref: bool = True) -> None:
-    """Build the checkers with oracle/Makefile (the reference only if its sources exist)."""
-    targets = ["oracle", "ref"] if ref else ["oracle"]
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+EXAMPLES_DIR = os.path.join(HERE, "_ref", "examples")
+
+
+def build(ref: bool = True, ref_root: str | None = None) -> None:
+    """Build the checkers with oracle/Makefile.
+
+    With ``ref``, also the reference build and its example programs, from the reference checkout
+    ``ref_root`` (default: the environment variable TLIBTTM_REF_ROOT); without one, prebuilt
+    copies under oracle/_ref are kept."""
+    targets = ["oracle", "ref", "examples"] if ref else ["oracle"]
+    root = ref_root if ref_root is not None else os.environ.get("TLIBTTM_REF_ROOT", "")
+    subprocess.run(["make", "-s", "-C", HERE] + targets + ([f"REF_ROOT={root}"] if root else []), check=True)
 
 
 def _sz(v):

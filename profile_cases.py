@@ -1,6 +1,7 @@
-"""One TTM case through the C ABI, repeated: the case runner used for ncu captures.
+"""One TTM case through the C ABI, repeated: the measurement driver the ncu captures under
+profiles/ run.
 
-    python -m ttm_b200.profile_cases --dtype f32 --precision bf16x3 --na 256,256,256,16 --q 2 \
+    python profile_cases.py --dtype f32 --precision bf16x3 --na 256,256,256,16 --q 2 \
         --m 256 [--pia 1,2,3,4] [--iters 3]
 
 A (extents `na`, layout `pia`, dense) and B (m x n_q, column-major) are N(0,1) on the device,
@@ -11,8 +12,11 @@ from __future__ import annotations
 
 import argparse
 import math
+import os
+import sys
 
-from . import _lib
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from ttm_b200 import _lib  # noqa: E402
 
 
 def _dense(n, pi):

@@ -6,7 +6,6 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
-REF_ROOT = "/root/reference"
 
 
 def pytest_configure(config):
@@ -33,7 +32,7 @@ def oracle_c():
 @pytest.fixture(scope="session")
 def reference():
     from oracle import Reference, REF_SO
-    if not os.path.exists(REF_SO) and not os.path.isdir(os.path.join(REF_ROOT, "include")):
+    if not os.path.exists(REF_SO):
         pytest.skip("reference build (oracle/_ref) not available")
     try:
         return Reference()

@@ -123,6 +123,29 @@ def test_small_tuning_run(cuda):
         assert r["regret_mlp_with_fallback"] < 0.5
 
 
+def test_shipped_selector_gains_over_the_heuristic_on_held_out_problems(cuda):
+    """The network shipped in ttm_b200/schedule_model.json, on the 2,000 held-out problems (seed 2,
+    float and double, drawn as in training), timed here by the exhaustive autotuner: its time
+    regret is within 5 % of the autotuned time with and without the autotuner fallback, below the
+    regret of the planner's fixed heuristic (the method without the network), and the fallback
+    decides for fewer than a third of the problems."""
+    import json
+    from ttm_b200 import selector, workloads
+    with open(selector.MODEL_PATH) as f:
+        shipped = json.load(f)
+    model = selector.MLP.from_json(shipped["model"])
+    test = selector.with_dtypes(workloads.problems(2000, 2), 2)
+    res = selector.evaluate(model, selector.DtypeTuner(), test, margin=shipped["evaluation"]["margin"])
+    assert 0.3 < res["f64_share"] < 0.7
+    for k in ("exact", "fp32_accurate"):
+        r = res[k]
+        assert r["regret_mlp_with_fallback"] <= 0.05, (k, r)
+        assert r["regret_mlp_alone"] <= 0.05, (k, r)
+        assert r["regret_mlp_with_fallback"] < r["regret_heuristic"], (k, r)
+        assert r["regret_mlp_alone"] < r["regret_heuristic"], (k, r)
+        assert r["fallback_rate"] < 1.0 / 3.0, (k, r)
+
+
 def test_tuned_precision_uses_the_shipped_model(cuda):
     import torch
     from ttm_b200 import ttmpy as tp

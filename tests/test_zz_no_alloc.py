@@ -72,6 +72,67 @@ def test_noalloc_matches_existing_entry_point_twice(cuda):
         assert err <= TOL, (na, q, m, err)
 
 
+def test_noalloc_matches_the_oracle(cuda, oracle_c):
+    """Against the C oracle (FP64 accumulation of the float inputs), not only against the other
+    entry point of the same kernel; m = 272 > 256 takes two 256-column blocks of B (a 1 MiB image,
+    exactly the limit)."""
+    import torch
+    stream = torch.cuda.current_stream().cuda_stream
+    L = _lib.lib()
+    for na, pia, q, m, b_cm, seed in (([64, 48, 40], [2, 1, 3], 1, 40, True, 4),
+                                      ([40, 512, 24], [1, 2, 3], 2, 272, False, 5)):
+        a, b, md = _problem(cuda, na, pia, q, m, b_cm, seed)
+        c = torch.full((int(np.prod(md["nc"])),), float("nan"), device=cuda)
+        rc = _call("tlibttm_ttm_f32_bf16x3_noalloc", q, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream)
+        assert rc == 0, L.tlibttm_last_error()
+        assert L.tlibttm_synchronize(C.c_void_p(stream)) == 0, L.tlibttm_last_error()
+        ha, hb = a.cpu().numpy(), b.cpu().numpy()
+        want = np.zeros(int(np.prod(md["nc"])), dtype=np.float32)
+        oracle_c.ttm(q, ha, md["na"], md["wa"], md["pia"], hb, md["nb"], md["pib"], want, md["nc"], md["wc"])
+        got = c.double().cpu().numpy()
+        err = np.linalg.norm(got - want) / np.linalg.norm(want)
+        assert err <= TOL, (na, q, m, err)
+
+
+def _pool_used_high(dev_index):
+    """High watermark of the device's default stream-ordered pool (cudaMallocAsync), through the
+    CUDA runtime that torch loaded."""
+    rt = C.CDLL("libcudart.so.12")
+    pool = C.c_void_p()
+    assert rt.cudaDeviceGetDefaultMemPool(C.byref(pool), C.c_int(dev_index)) == 0
+    val = C.c_uint64(0)
+    assert rt.cudaMemPoolGetAttribute(pool, C.c_int(8), C.byref(val)) == 0   # cudaMemPoolAttrUsedMemHigh
+    return rt, pool, val.value
+
+
+def test_noalloc_allocates_nothing(cuda):
+    """The pool's high watermark is reset, the entry point runs twice, and the watermark has not
+    moved; the allocating bf16x3 path then moves it, which shows that the check sees allocations."""
+    import torch
+    L = _lib.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    a, b, md = _problem(cuda, [256, 64, 40], [1, 2, 3], 2, 256, True, 6)
+    c = torch.empty(int(np.prod(md["nc"])), device=cuda)
+    # first call on this device (its one-time symbol lookup) outside the measured window
+    assert _call("tlibttm_ttm_f32_bf16x3_noalloc", 2, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream) == 0
+    torch.cuda.synchronize()
+    rt, pool, _ = _pool_used_high(cuda.index or 0)
+    assert rt.cudaMemPoolSetAttribute(pool, C.c_int(8), C.byref(C.c_uint64(0))) == 0   # reset to current use
+    _, _, before = _pool_used_high(cuda.index or 0)
+    for _ in range(2):
+        rc = _call("tlibttm_ttm_f32_bf16x3_noalloc", 2, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream)
+        assert rc == 0, L.tlibttm_last_error()
+    assert L.tlibttm_synchronize(C.c_void_p(stream)) == 0
+    _, _, after = _pool_used_high(cuda.index or 0)
+    assert after == before
+    rc = _call("tlibttm_ttm_ex", 2, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream,
+               extra=(_lib.F32, _lib.PREC_BF16X3))
+    assert rc == 0, L.tlibttm_last_error()
+    assert L.tlibttm_synchronize(C.c_void_p(stream)) == 0
+    _, _, grown = _pool_used_high(cuda.index or 0)
+    assert grown > before
+
+
 def test_noalloc_rejects_what_it_cannot_hold(cuda):
     import torch
     L = _lib.lib()
@@ -82,6 +143,12 @@ def test_noalloc_rejects_what_it_cannot_hold(cuda):
     rc = _call("tlibttm_ttm_f32_bf16x3_noalloc", 1, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream)
     assert rc == _lib.ERR_ARG
     assert "at most 1048576 bytes" in L.tlibttm_last_error().decode()
+    # m = 272 > 256 pads B to two 256-column blocks: with n_q = 544 the image is 1,114,112 bytes
+    a, b, md = _problem(cuda, [544, 40], [1, 2], 1, 272, True, 7)
+    c = torch.empty(272 * 40, device=cuda)
+    rc = _call("tlibttm_ttm_f32_bf16x3_noalloc", 1, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream)
+    assert rc == _lib.ERR_ARG
+    assert "1114112-byte" in L.tlibttm_last_error().decode()
     # host operands would need staging buffers
     na, pia, q, m = [64, 32, 8], [1, 2, 3], 2, 32
     ha = np.zeros(64 * 32 * 8, dtype=np.float32)

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(PKG, "libtlibttm_cuda.so")
 OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_UNSUPPORTED, ERR_DEVICE = range(6)
 F32, F64 = 0, 1
 PREC_DEFAULT, PREC_PLAIN, PREC_BF16X3, PREC_FP8, PREC_OZAKI, PREC_AUTO = range(6)
+INJECT_NONE, INJECT_FAIL_ALLOC, INJECT_WAIT_NS, INJECT_SKIP_B_STAGE = range(4)
 PRECISIONS = {"default": PREC_DEFAULT, "plain": PREC_PLAIN, "bf16x3": PREC_BF16X3, "fp8": PREC_FP8,
               "ozaki": PREC_OZAKI, "auto": PREC_AUTO}
 
@@ -58,6 +59,8 @@ def _declare(L):
     L.tlibttm_inverse_mode.argtypes = [_SZ, C.c_size_t, C.c_size_t]
     L.tlibttm_strides.restype = C.c_int
     L.tlibttm_strides.argtypes = [_SZ, C.c_size_t, _SZ, _SZ]
+    L.tlibttm_inject.restype = C.c_int
+    L.tlibttm_inject.argtypes = [C.c_int, C.c_longlong]
 
 
 def lib():
@@ -137,3 +140,8 @@ def strides(shape, layout):
     out = (C.c_size_t * len(shape))()
     check(lib().tlibttm_strides(sz(shape), len(shape), sz(layout), out))
     return list(out)
+
+
+def inject(what: int, arg: int = 0) -> None:
+    """Host-side fault injection for failure-detection tests (tlibttm_inject)."""
+    check(lib().tlibttm_inject(int(what), int(arg)))

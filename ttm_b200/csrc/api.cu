@@ -43,6 +43,22 @@ const char* kernel_name(int id)
 }
 
 namespace {
+bool injected_alloc_failure();
+}
+
+cudaError_t dev_malloc(void** p, size_t bytes)
+{
+    if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t s)
+{
+    if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
+    return cudaMallocAsync(p, bytes, s);
+}
+
+namespace {
 
 thread_local std::string g_err;
 thread_local const char* g_last_kernel = "";
@@ -71,7 +87,22 @@ int fail(int code, const std::string& msg)
 int cuda_fail(cudaError_t e, const char* where)
 {
     g_err = std::string("tlibttm: CUDA error in ") + where + ": " + cudaGetErrorString(e);
-    return TLIBTTM_ERR_CUDA;
+    return e == cudaErrorMemoryAllocation ? TLIBTTM_ERR_ALLOC : TLIBTTM_ERR_CUDA;
+}
+
+// Host-side fault injection (tlibttm_inject): the allocation that fails next, the wait bound of
+// the bf16x3 kernel and the one-shot skipped B stage.
+std::atomic<long long> g_fail_alloc_in{0};
+std::atomic<unsigned long long> g_wait_ns{0};
+std::atomic<int> g_skip_b{0};
+
+bool injected_alloc_failure()
+{
+    long long n = g_fail_alloc_in.load();
+    while (n > 0) {
+        if (g_fail_alloc_in.compare_exchange_weak(n, n - 1)) return n == 1;
+    }
+    return false;
 }
 
 struct Args {
@@ -235,7 +266,12 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s, int64_t s
     }
     if (precision == TLIBTTM_PREC_OZAKI && x.dtype != TLIBTTM_F64)
         return fail(TLIBTTM_ERR_UNSUPPORTED, "tlibttm: the ozaki precision takes double operands.");
-    if ((precision == TLIBTTM_PREC_FP8 || precision == TLIBTTM_PREC_OZAKI) && tc8_supported(v, precision, x.dtype)) {
+    if (precision == TLIBTTM_PREC_FP8 || precision == TLIBTTM_PREC_OZAKI) {
+        // an explicit 8-bit request never falls back to other arithmetic silently
+        if (!tc8_supported(v, precision, x.dtype))
+            return fail(TLIBTTM_ERR_UNSUPPORTED, precision == TLIBTTM_PREC_OZAKI
+                                                     ? "tlibttm: the ozaki path takes n_q <= 16384 (exact int32 sums)."
+                                                     : "tlibttm: the fp8 path cannot run this problem.");
         int kid = K_NONE, n = 0;
         cudaError_t e = launch_tc8(v, precision, x.dtype, s, &kid, &n);
         if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);   // exponent and slicer kernels
@@ -281,7 +317,7 @@ cudaError_t ensure(DevBuf& b, size_t bytes)
         b.bytes = 0;
         if (e != cudaSuccess) return e;
     }
-    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    cudaError_t e = dev_malloc(&b.ptr, bytes);
     if (e == cudaSuccess) b.bytes = bytes;
     return e;
 }
@@ -552,10 +588,20 @@ int launches_of(const Single& sg, int dtype, int precision)
     int pr = precision == TLIBTTM_PREC_DEFAULT ? g_precision.load() : precision;
     if (pr == TLIBTTM_PREC_AUTO)
         pr = (dtype == TLIBTTM_F32 && tc_supported(sg.pl.v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3 : TLIBTTM_PREC_PLAIN;
+    if (pr == TLIBTTM_PREC_FP8 || pr == TLIBTTM_PREC_OZAKI) return tc8_launches(sg.pl.v, pr);
     return (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) ? 2 : 1;
 }
 
 }  // namespace
+
+unsigned long long wait_limit_ns()
+{
+    const unsigned long long v = g_wait_ns.load();
+    return v ? v : 4000000000ull;
+}
+
+bool take_skip_b() { return g_skip_b.exchange(0) != 0; }
+
 }  // namespace tlibttm
 
 struct tlibttm_plan_s {
@@ -784,7 +830,8 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
         return fail(TLIBTTM_ERR_ARG, "tlibttm_ttm_f32_bf16x3_noalloc: B needs a " + std::to_string(tc_image_bytes(v)) +
                                          "-byte split image; this entry point holds at most " +
                                          std::to_string(kNoAllocImageBytes) +
-                                         " bytes (ceil(m/16)*16 * ceil(n_q/32)*32 * 4 bytes, e.g. m = 256 with n_q <= 1024).");
+                                         " bytes (cols(m) * ceil(n_q/32)*32 * 4 bytes, cols(m) = ceil(m/16)*16 for m <= 256, "
+                                         "else ceil(m/256)*256; e.g. m = 256 with n_q <= 1024).");
     int kid = K_NONE;
     e = launch_tc_noalloc(v, static_cast<cudaStream_t>(stream), &kid);
     if (e == cudaSuccess) ++g_launches;   // split_b_kernel; note_launch counts the main kernel
@@ -832,6 +879,16 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                     v.c = x.c;
                     bool single = false;
                     const int64_t elems = v.outer * v.inner * v.nq;
+                    if (pl.dense && v.m > kSmallM && (prec == TLIBTTM_PREC_FP8 || prec == TLIBTTM_PREC_OZAKI)) {
+                        // the 8-bit paths run as their own launches; a problem they cannot run is an error
+                        if (!tc8_supported(v, prec, dtype)) {
+                            rc = fail(TLIBTTM_ERR_UNSUPPORTED, prec == TLIBTTM_PREC_FP8
+                                                                   ? "the fp8 precision takes float operands."
+                                                                   : "the ozaki precision takes double operands with n_q <= 16384.");
+                            return fail(rc, problem_prefix(i) + g_err);
+                        }
+                        single = true;
+                    }
                     if (pl.dense && v.m > kSmallM && dtype == TLIBTTM_F32) {
                         // bf16x3 asked for explicitly: every supported problem takes it; under auto,
                         // supported problems above the single-launch size
@@ -906,8 +963,8 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
     }
     P->total = first;
     if (!P->descs.empty()) {
-        if ((e = cudaMalloc(&P->d_desc, P->descs.size() * sizeof(GroupDesc))) != cudaSuccess ||
-            (e = cudaMalloc(&P->d_queue, sizeof(unsigned long long))) != cudaSuccess)
+        if ((e = dev_malloc(reinterpret_cast<void**>(&P->d_desc), P->descs.size() * sizeof(GroupDesc))) != cudaSuccess ||
+            (e = dev_malloc(reinterpret_cast<void**>(&P->d_queue), sizeof(unsigned long long))) != cudaSuccess)
             return fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_batched: device allocation failed.");
         if ((e = cudaMemcpy(P->d_desc, P->descs.data(), P->descs.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice)) != cudaSuccess)
             return cuda_fail(e, "plan upload");
@@ -958,7 +1015,7 @@ int tlibttm_plan_chain(int dtype, int precision, unsigned p, const void* a, cons
     }
     if (count > 1) {
         for (int i = 0; i < 2; ++i)
-            if ((e = cudaMalloc(&P->bufs[i], std::max<size_t>(max_mid, 1) * es)) != cudaSuccess)
+            if ((e = dev_malloc(&P->bufs[i], std::max<size_t>(max_mid, 1) * es)) != cudaSuccess)
                 return fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_chain: device allocation failed.");
     }
     const void* in = a;
@@ -1053,6 +1110,30 @@ int tlibttm_plan_destroy(tlibttm_plan* plan)
 {
     plan_free(plan);
     return TLIBTTM_OK;
+}
+
+int tlibttm_inject(int what, long long arg)
+{
+    switch (what) {
+    case TLIBTTM_INJECT_NONE:
+        g_fail_alloc_in = 0;
+        g_wait_ns = 0;
+        g_skip_b = 0;
+        return TLIBTTM_OK;
+    case TLIBTTM_INJECT_FAIL_ALLOC:
+        if (arg < 0) return fail(TLIBTTM_ERR_ARG, "tlibttm_inject: the allocation count must be >= 0.");
+        g_fail_alloc_in = arg;
+        return TLIBTTM_OK;
+    case TLIBTTM_INJECT_WAIT_NS:
+        if (arg < 0) return fail(TLIBTTM_ERR_ARG, "tlibttm_inject: the wait bound must be >= 0.");
+        g_wait_ns = (unsigned long long)arg;
+        return TLIBTTM_OK;
+    case TLIBTTM_INJECT_SKIP_B_STAGE:
+        g_skip_b = arg ? 1 : 0;
+        return TLIBTTM_OK;
+    default:
+        return fail(TLIBTTM_ERR_ARG, "tlibttm_inject: unknown injection.");
+    }
 }
 
 const char* tlibttm_last_error(void) { return g_err.c_str(); }

@@ -118,4 +118,15 @@ constexpr int64_t kSmallM = 16;
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Every device allocation of the library goes through these two wrappers (cudaMalloc and the
+// stream-ordered cudaMallocAsync), so that a test can make the n-th one fail (tlibttm_inject).
+cudaError_t dev_malloc(void** p, size_t bytes);
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t s);
+
+// Bound of the bounded mbarrier waits of the bf16x3 kernel, in ns (4 s unless a test set it).
+unsigned long long wait_limit_ns();
+// True once after a test asked for it: the next bf16x3 launch's B producer skips its first
+// stage (no copy, no arrive), so that the MMA issuer's bounded wait runs out.
+bool take_skip_b();
+
 }  // namespace tlibttm

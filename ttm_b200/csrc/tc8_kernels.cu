@@ -502,6 +502,15 @@ bool tc8_supported(const View3& v, int precision, int dtype)
     return plan8(v, precision, p);
 }
 
+int tc8_launches(const View3& v, int precision)
+{
+    Plan8 p;
+    if (!plan8(v, precision, p)) return 0;
+    const int64_t rows = v.outer * v.inner;
+    const int64_t chunk = std::min<int64_t>(p.chunk_rows, ((rows + kRows - 1) / kRows) * kRows);
+    return (int)(2 + 3 * ((rows + chunk - 1) / chunk));   // B exponents + slicer, then per chunk three
+}
+
 cudaError_t launch_tc8(const View3& v, int precision, int dtype, cudaStream_t s, int* kid, int* launches)
 {
     *launches = 0;
@@ -535,7 +544,7 @@ cudaError_t launch_tc8(const View3& v, int precision, int dtype, cudaStream_t s,
     auto up = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t total = up(brows * sizeof(int)) + up(bimg_bytes) + up(chunk * sizeof(int)) + up(aimg_bytes);
     uint8_t* scratch = nullptr;
-    if ((e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), total, s)) != cudaSuccess) return e;
+    if ((e = dev_malloc_async(reinterpret_cast<void**>(&scratch), total, s)) != cudaSuccess) return e;
     int* bexp = reinterpret_cast<int*>(scratch);
     uint8_t* bimg = scratch + up(brows * sizeof(int));
     int* aexp = reinterpret_cast<int*>(bimg + up(bimg_bytes));

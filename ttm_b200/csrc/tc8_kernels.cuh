@@ -14,4 +14,7 @@ bool tc8_supported(const View3& v, int precision, int dtype);
 // number of kernels enqueued.
 cudaError_t launch_tc8(const View3& v, int precision, int dtype, cudaStream_t s, int* kid, int* launches);
 
+// Kernels launch_tc8 enqueues for this view (0 when the path cannot run it).
+int tc8_launches(const View3& v, int precision);
+
 }  // namespace tlibttm

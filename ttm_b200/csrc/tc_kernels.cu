@@ -105,6 +105,8 @@ struct TcParams {
     int fstages;             // A ring depth (FP32 tile, converted in place)
     int ostages;             // B ring depth
     int tma_c;               // epilogue stores C through the C tensor map
+    int skip_b;              // test of the bounded waits: the B producer skips its first stage
+    unsigned long long wait_ns;   // bound of the pipeline's mbarrier waits
 };
 
 // Shared memory: [A ring][B ring][epilogue staging][barriers]. An A stage holds kSub FP32
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 const int64_t mt = t % P.tiles_m;
                 for (int st = 0; st < kstages; ++st) {
-                    if (!mbar_wait(&a_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(&a_empty[s], ph ^ 1, abort_flag, P.wait_ns)) { ok = false; break; }
                     if (P.ldg_a) {
                         // no copy: the stage is free for the converters, which load A themselves
                         mbar_arrive(&a_full[s]);
@@ -270,7 +272,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
                 const int64_t jb = t / P.tiles_m;
                 for (int st = 0; st < kstages; ++st) {
-                    if (!mbar_wait(&b_empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(&b_empty[s], ph ^ 1, abort_flag, P.wait_ns)) { ok = false; break; }
+                    if (P.skip_b && t == blockIdx.x && st == 0) {
+                        // test of the bounded waits: this stage is never filled (no copy, no arrive)
+                        if (++s == BS) { s = 0; ph ^= 1; }
+                        continue;
+                    }
                     issued[s] = (int)ph;
                     mbar_expect_tx(&b_full[s], L.bstage_bytes);
                     // the image holds kstages * kSub sub-blocks per j block: one copy per stage
@@ -300,11 +307,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t cph = 0;
             bool ok = true;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                if (!mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag)) break;
+                if (!mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag, P.wait_ns)) break;
                 tc_fence_after();
                 const uint32_t dcol = tmem_base + (uint32_t)(ab * P.nt);
                 for (int st = 0; st < kstages; ++st) {
-                    if (!mbar_wait(&b_full[bs], bph, abort_flag) || !mbar_wait(&a_conv[as], aph, abort_flag)) {
+                    if (!mbar_wait(&b_full[bs], bph, abort_flag, P.wait_ns) || !mbar_wait(&a_conv[as], aph, abort_flag, P.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -353,7 +360,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if ((int)(n % kConvGroups) != g) continue;
                 const int s = (int)(n % AS);
                 const uint32_t ph = (uint32_t)((n / AS) & 1);
-                const bool got = ok && mbar_wait(&a_full[s], ph, abort_flag);
+                const bool got = ok && mbar_wait(&a_full[s], ph, abort_flag, P.wait_ns);
                 const bool have = __all_sync(0xffffffffu, got);
                 if (!have) ok = false;
 #pragma unroll 1
@@ -437,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         int ab = 0;
         uint32_t aph = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-            if (!mbar_wait(&acc_full[ab], aph, abort_flag)) break;
+            if (!mbar_wait(&acc_full[ab], aph, abort_flag, P.wait_ns)) break;
             tc_fence_after();
             const int64_t jb = t / P.tiles_m, mt = t - jb * P.tiles_m;
             int64_t k, r0;            // slice and first row (i for GEOM_MN, k for GEOM_K) of this warp
@@ -945,7 +952,7 @@ cudaError_t state_for(int dev, DevState*& out)
     std::lock_guard<std::mutex> lk(g_state_mu);
     DevState& d = g_state[dev];
     if (!d.status) {
-        cudaError_t e = cudaMalloc(&d.status, 256);
+        cudaError_t e = dev_malloc(reinterpret_cast<void**>(&d.status), 256);
         if (e != cudaSuccess) return e;
         e = cudaMemset(d.status, 0, 256);
         if (e != cudaSuccess) return e;
@@ -1106,6 +1113,8 @@ cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaS
     P.jblocks = jblocks;
     P.kchunks = kchunks;
     P.kstages = kstages;
+    P.wait_ns = wait_limit_ns();
+    P.skip_b = take_skip_b() ? 1 : 0;
     size_t smem = 0;
     if (!choose_stages(nt, P.fstages, P.ostages, smem)) return cudaErrorNotSupported;
 
@@ -1442,7 +1451,7 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
     void* scratch = nullptr;
     if (sh.S > 1) {
         const size_t ws = (sh.ws_bytes + 255) & ~size_t(255);
-        if ((e = cudaMallocAsync(&scratch, ws + (size_t)sh.tiles * sizeof(unsigned), s)) != cudaSuccess) return e;
+        if ((e = dev_malloc_async(&scratch, ws + (size_t)sh.tiles * sizeof(unsigned), s)) != cudaSuccess) return e;
         P.ws = scratch;
         P.cnt = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(scratch) + ws);
         e = cudaMemsetAsync(P.cnt, 0, (size_t)sh.tiles * sizeof(unsigned), s);
@@ -1493,7 +1502,7 @@ cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid)
     DevState* st = nullptr;
     if ((e = state_for(dev, st)) != cudaSuccess) return e;
     void* img = nullptr;
-    if ((e = cudaMallocAsync(&img, tc_image_bytes(v), s)) != cudaSuccess) return e;
+    if ((e = dev_malloc_async(&img, tc_image_bytes(v), s)) != cudaSuccess) return e;
     e = run_bf16x3(v, static_cast<uint8_t*>(img), st->status, g_sm_count, s);
     cudaFreeAsync(img, s);
     return e;

@@ -30,7 +30,8 @@ int tc_read_status();
 cudaError_t tc_status_word(int dev, int** out);
 
 // Largest pre-split B image the allocation-free bf16x3 variant can hold (bytes):
-// ceil(m/16)*16 * ceil(n_q/16)*16 * 4 <= 1 MiB for m <= 256, e.g. m = 256 with n_q <= 1024.
+// cols(m) * ceil(n_q/32)*32 * 4 bytes, cols(m) = ceil(m/16)*16 for m <= 256 and ceil(m/256)*256
+// above (whole 256-row blocks of B), e.g. m = 256 with n_q <= 1024.
 constexpr size_t kNoAllocImageBytes = size_t(1) << 20;
 
 // Bytes of the pre-split B image a bf16x3 launch of this view needs.

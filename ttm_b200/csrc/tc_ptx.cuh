@@ -46,14 +46,16 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase)
 }
 
 // Bounded wait: false when the CTA is aborting or this wait expired (which starts the abort).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag)
+// `limit_ns` is the bound (kernels that take it as a launch parameter let a test shorten it).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag,
+                                          unsigned long long limit_ns = kTimeoutNs)
 {
     if (mbar_try(bar, phase)) return true;
     const unsigned long long t0 = gtimer();
     while (true) {
         if (mbar_try(bar, phase)) return true;
         if (*abort_flag) return false;
-        if (gtimer() - t0 > kTimeoutNs) {
+        if (gtimer() - t0 > limit_ns) {
             *abort_flag = 1;
             return false;
         }

@@ -96,7 +96,19 @@ def features(pr, dtype_id=_lib.F32):
     return f
 
 
-def valid_mask(pr, dtype_id=_lib.F32):
+def dtype_of(pr) -> int:
+    """The I/O type of a problem (float unless the problem says otherwise)."""
+    return int(pr.get("dtype", _lib.F32))
+
+
+def with_dtypes(probs, seed, f64_share=0.5):
+    """Marks about `f64_share` of the problems double (seeded, independent of the shapes)."""
+    rng = np.random.default_rng(10_000 + seed)
+    return [dict(pr, dtype=_lib.F64 if rng.random() < f64_share else _lib.F32) for pr in probs]
+
+
+def valid_mask(pr, dtype_id=None):
+    dtype_id = dtype_of(pr) if dtype_id is None else dtype_id
     L = lib()
     na, pia = _lib.sz(pr["na"]), _lib.sz(pr["pia"])
     return [bool(L.tlibttm_schedule_valid(dtype_id, s, pr["q"], pr["p"], na, pia, pr["m"])) for s in range(1, NS + 1)]
@@ -155,6 +167,20 @@ class Autotuner:
             out.append(float(np.median([e0.elapsed_time(e1) * 1e3 for e0, e1 in evs])))
         self.db[k] = out
         return out
+
+
+class DtypeTuner:
+    """One Autotuner per I/O type; each problem is timed in its own type (`dtype` key)."""
+
+    def __init__(self, reps=3, cap=workloads.CAP):
+        self.tuners = {_lib.F32: Autotuner(reps=reps, cap=cap, dtype_id=_lib.F32),
+                       _lib.F64: Autotuner(reps=reps, cap=cap, dtype_id=_lib.F64)}
+
+    def times(self, pr):
+        return self.tuners[dtype_of(pr)].times(pr)
+
+    def best(self, pr, allowed=None):
+        return self.tuners[dtype_of(pr)].best(pr, allowed)
 
     def best(self, pr, allowed=None):
         t = self.times(pr)
@@ -268,7 +294,8 @@ class Selector:
         self.tuner = tuner
         self.margin = margin
 
-    def choose(self, pr, allowed, dtype_id=_lib.F32):
+    def choose(self, pr, allowed, dtype_id=None):
+        dtype_id = dtype_of(pr) if dtype_id is None else dtype_id
         ok = valid_mask(pr, dtype_id)
         # a model trained before a schedule existed never proposes it
         cands = [s for s in range(1, NS + 1) if ok[s - 1] and s in allowed and s <= self.model.dims[-1]]
@@ -284,13 +311,13 @@ class Selector:
         return ranked[0], False
 
 
-def dataset(tuner, probs, dtype_id=_lib.F32, log=None):
+def dataset(tuner, probs, log=None):
     X, T, M = [], [], []
     for n, pr in enumerate(probs):
         if log and n and n % 2000 == 0:
             log(f"timed {n} problems")
         t = tuner.times(pr)
-        X.append(features(pr, dtype_id))
+        X.append(features(pr, dtype_of(pr)))
         T.append([math.log2(x) if x is not None else 0.0 for x in t])
         M.append([1.0 if x is not None else 0.0 for x in t])
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -315,15 +342,24 @@ def regret(tuner, probs, choose, allowed):
 def train_and_evaluate(n_train, n_test, steps=3000, seed_train=1, seed_test=2, margin=0.15, log=print,
                        cap=workloads.CAP):
     t0 = time.time()
-    tuner = Autotuner(cap=cap)
-    train = workloads.problems(n_train, seed_train, cap=cap)
-    test = workloads.problems(n_test, seed_test, cap=cap)
+    tuner = DtypeTuner(cap=cap)
+    train = with_dtypes(workloads.problems(n_train, seed_train, cap=cap), seed_train)
+    test = with_dtypes(workloads.problems(n_test, seed_test, cap=cap), seed_test)
     X, T, M = dataset(tuner, train, log=log)
     log(f"timed {n_train} training problems in {time.time() - t0:.0f} s")
     model = MLP().fit(X, T, M, steps=steps, log=log)
+    out = {"n_train": n_train, "n_test": n_test, "steps": steps, "margin": margin}
+    out.update(evaluate(model, tuner, test, margin=margin))
+    out["seconds"] = time.time() - t0
+    return model, out
+
+
+def evaluate(model, tuner, test, margin=0.15):
+    """Held-out regret of the network with and without the autotuner fallback, and of the
+    planner's fixed heuristic (the method without the network), per schedule set."""
     dataset(tuner, test)
     allowed_sets = {"exact": set(EXACT), "fp32_accurate": set(range(1, NS + 1))}
-    out = {"n_train": n_train, "n_test": n_test, "steps": steps, "margin": margin}
+    out = {"f64_share": sum(dtype_of(p) == _lib.F64 for p in test) / max(len(test), 1)}
     for name, allowed in allowed_sets.items():
         sel = Selector(model, tuner, margin=margin)
         fallbacks = [0]
@@ -342,20 +378,20 @@ def train_and_evaluate(n_train, n_test, steps=3000, seed_train=1, seed_test=2, m
                      "fallback_rate": fallbacks[0] / len(test),
                      "regret_mlp_alone": r_nofb[0], "geomean_regret_mlp_alone": r_nofb[1],
                      "regret_heuristic": r_heur[0], "geomean_regret_heuristic": r_heur[1]}
-    out["seconds"] = time.time() - t0
-    return model, out
+    return out
 
 
 def _heuristic_in(pr, allowed):
     """The planner's default choice for a problem (plain for 'exact', auto for 'fp32_accurate')."""
     inner, nq, outer = geometry(pr["na"], pr["pia"], pr["q"])
+    es = 4 if dtype_of(pr) == _lib.F32 else 8
     if pr["m"] <= 16:
         if inner == 1:
-            big = math.prod(pr["na"]) * 4 >= 64 << 20
+            big = math.prod(pr["na"]) * es >= 64 << 20
             return 6 if (6 in allowed and big and nq > 16 and valid_mask(pr)[5]) else 4
-        if 6 in allowed and math.prod(pr["na"]) * 4 >= 64 << 20 and valid_mask(pr)[5]:
+        if 6 in allowed and math.prod(pr["na"]) * es >= 64 << 20 and valid_mask(pr)[5]:
             return 6
-        rv = 4
+        rv = 16 // es
         w = rv if inner % rv == 0 else 1
         return 3 if math.ceil(inner * outer / (32 * w)) < 148 * 32 else 2
     if 5 in allowed and valid_mask(pr)[4]:

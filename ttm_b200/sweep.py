@@ -1,6 +1,7 @@
 """Layout/mode sweep: throughput of every case of the 2^26-element sweep on one GPU.
 
     python -m ttm_b200.sweep [--dtypes f32,f64] [--ms 1,8,64,512] [--layouts 10] [--out sweep.json]
+                             [--check [--samples 2048]] [--precision auto]
 
 A has prod(n) = 2^26 elements: the extent sets (512,256,512), (128,64,128,64), (32,32,64,32,32),
 (32,16,32,16,16,16) and two seeded random splits of the 26 bits over p = 3..6 modes (every
@@ -61,6 +62,41 @@ def layouts(p, count, seed):
     return out
 
 
+def view3(na, pia, q):
+    """(outer, n_q, inner) of the slice view of a tensor dense under layout pia."""
+    qh = pia.index(q)
+    inner = math.prod(na[pia[r] - 1] for r in range(qh))
+    outer = math.prod(na[pia[r] - 1] for r in range(qh + 1, len(na)))
+    return outer, na[q - 1], inner
+
+
+def sample_fibres(A, B, C, na, pia, q, m, count, gen, b_cm=True):
+    """Gathers `count` random output fibres: A_s (count x n_q) and C_s (count x m) as float64
+    numpy arrays, and B as a float64 (m x n_q) array. Each fibre is (k, i) of the slice view:
+    A_s[s, l] = A[k][l][i], C_s[s, j] = C[k][j][i]."""
+    import torch
+    outer, nq, inner = view3(na, pia, q)
+    n = outer * inner
+    idx = torch.randint(0, n, (min(count, n),), device=A.device, generator=gen) if count < n else \
+        torch.arange(n, device=A.device)
+    ks, iis = idx // inner, idx % inner
+    a_s = A.view(outer, nq, inner)[ks, :, iis].double().cpu().numpy()
+    c_s = C.view(outer, m, inner)[ks, :, iis].double().cpu().numpy()
+    b = B.double().cpu().numpy()
+    b = b.reshape(nq, m).T if b_cm else b.reshape(m, nq)
+    return a_s, b, c_s
+
+
+def fibre_errors(a_s, b, c_s):
+    """max|c - r| / max|r| and ||c - r|| / ||r|| over the sampled fibres, r = a_s b^T in FP64."""
+    import numpy as np
+    r = a_s @ b.T
+    d = c_s - r
+    rmax = float(np.max(np.abs(r))) or 1.0
+    rn = float(np.linalg.norm(r)) or 1.0
+    return float(np.max(np.abs(d))) / rmax, float(np.linalg.norm(d)) / rn
+
+
 def hbm_peak():
     path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
     try:
@@ -70,7 +106,11 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def sweep(dtypes=("f32", "f64"), ms=(1, 8, 64, 512), n_layouts=10, reps=10, seed=0, log=print):
+def sweep(dtypes=("f32", "f64"), ms=(1, 8, 64, 512), n_layouts=10, reps=10, seed=0, log=print, check=False,
+          samples=2048, precision=None):
+    """Times every case; with `check`, also compares `samples` sampled output fibres per case with
+    FP64 dot products (fields max_rel and rms_rel). `precision` is a key of _lib.PRECISIONS (the
+    library default when None)."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream(dev)
@@ -100,8 +140,10 @@ def sweep(dtypes=("f32", "f64"), ms=(1, 8, 64, 512), n_layouts=10, reps=10, seed
                         B = torch.randn(m * nq, device=dev, dtype=tdt, generator=gen)
                         C = torch.empty(nout, device=dev, dtype=tdt)
 
+                        prec = _lib.PRECISIONS[precision] if precision else _lib.PREC_DEFAULT
+
                         def run():
-                            _lib.ttm_raw(dt, _lib.PREC_DEFAULT, q, p, A.data_ptr(), na, wa, pia, B.data_ptr(),
+                            _lib.ttm_raw(dt, prec, q, p, A.data_ptr(), na, wa, pia, B.data_ptr(),
                                          [m, nq], [1, 2], C.data_ptr(), nc, wc, stream.cuda_stream)
 
                         run()
@@ -118,6 +160,9 @@ def sweep(dtypes=("f32", "f64"), ms=(1, 8, 64, 512), n_layouts=10, reps=10, seed
                         gbs = es * (n + nout + m * nq) / t / 1e9
                         row = {"dtype": dname, "na": na, "pia": pia, "q": q, "m": m, "kernel": kernel,
                                "ms": 1e3 * t, "gbs": gbs, "hbm_frac": gbs / peak, "tflops": 2.0 * m * n / t / 1e12}
+                        if check:
+                            a_s, b_s, c_s = sample_fibres(A, B, C, na, pia, q, m, samples, gen)
+                            row["max_rel"], row["rms_rel"] = fibre_errors(a_s, b_s, c_s)
                         out["cases"].append(row)
                         del B, C
         del A
@@ -143,6 +188,9 @@ def summarize(cases):
             s[f"{dname}_m{m}"] = {"cases": len(rows), "hbm_frac_min": fr[0], "hbm_frac_median": fr[len(fr) // 2],
                                   "hbm_frac_max": fr[-1], "at_least_85pct": sum(f >= 0.85 for f in fr) / len(fr),
                                   "tflops_median": tf[len(tf) // 2], "kernels": kernels}
+            if all("rms_rel" in c for c in rows):
+                s[f"{dname}_m{m}"]["max_rel_worst"] = max(c["max_rel"] for c in rows)
+                s[f"{dname}_m{m}"]["rms_rel_worst"] = max(c["rms_rel"] for c in rows)
     return s
 
 
@@ -163,9 +211,13 @@ def main():
     ap.add_argument("--layouts", type=int, default=10)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--check", action="store_true", help="compare sampled fibres with FP64 dot products")
+    ap.add_argument("--samples", type=int, default=2048)
+    ap.add_argument("--precision", default=None)
     a = ap.parse_args()
     torch.cuda.set_device(0)
-    res = sweep(a.dtypes.split(","), [int(x) for x in a.ms.split(",")], a.layouts, a.reps)
+    res = sweep(a.dtypes.split(","), [int(x) for x in a.ms.split(",")], a.layouts, a.reps, check=a.check,
+                samples=a.samples, precision=a.precision)
     if a.out:
         with open(a.out, "w") as f:
             json.dump(res, f)
