@@ -146,10 +146,12 @@ enum tlibttm_schedule {
     TLIBTTM_SCHED_COLS = 2,        /* small-m kernel for strided fibres, rows spread over warps (m <= 16, inner >= 2) */
     TLIBTTM_SCHED_COLS_SPLIT = 3,  /* small-m kernel for strided fibres, l split over 8 warps (m <= 16, inner >= 2) */
     TLIBTTM_SCHED_ROWS = 4,        /* small-m kernel for contiguous fibres (m <= 16, q == pia[0]) */
-    TLIBTTM_SCHED_TC_BF16X3 = 5,   /* tensor-core bf16x3, float only (FP32-accurate, not exact; m > 16) */
+    TLIBTTM_SCHED_TC_BF16X3 = 5,   /* tensor-core bf16x3 on single SMs, float only (FP32-accurate, not exact; m > 16) */
     TLIBTTM_SCHED_COLS_TMA = 6,    /* small-m kernel fed by TMA (m <= 16): strided fibres (inner % 4 == 0), or
                                       contiguous fibres of >= 16 floats / 8 doubles on 16-byte boundaries */
-    TLIBTTM_SCHED_COUNT = 7
+    TLIBTTM_SCHED_TC_BF16X3_PAIR = 7, /* tensor-core bf16x3 on pairs of SMs with B in tensor memory, float only
+                                      (128 < m <= 256, n_q <= 256; inner >= 128 or q == pia[0]) */
+    TLIBTTM_SCHED_COUNT = 8
 };
 
 /* Runs one TTM with a given schedule (all operands device memory, A and C dense). */
@@ -251,8 +253,9 @@ int tlibttm_plan_destroy(tlibttm_plan* plan);
  *                   default of 4 s). On expiry the kernel's blocks stop, drain their own copies,
  *                   free tensor memory and raise the status word that tlibttm_synchronize (and
  *                   every blocking call) reports as TLIBTTM_ERR_DEVICE.
- *  SKIP_B_STAGE     arg != 0: the next bf16x3 launch never fills its first B stage, so that its
- *                   MMA issuer's bounded wait runs out (use with a short WAIT_NS).
+ *  SKIP_B_STAGE     arg != 0: the next bf16x3 launch never fills its first pipeline stage (the
+ *                   single-SM kernel's first B stage, the pair kernel's first A stage in its
+ *                   even CTA), so that the waits on it run out (use with a short WAIT_NS).
  */
 enum tlibttm_injection {
     TLIBTTM_INJECT_NONE = 0,

@@ -2,7 +2,7 @@
 profiles/ run.
 
     python profile_cases.py --dtype f32 --precision bf16x3 --na 256,256,256,16 --q 2 \
-        --m 256 [--pia 1,2,3,4] [--iters 3]
+        --m 256 [--pia 1,2,3,4] [--iters 3] [--schedule 7]
 
 A (extents `na`, layout `pia`, dense) and B (m x n_q, column-major) are N(0,1) on the device,
 C is allocated on the device; the call is made `iters` times on the current stream. Prints the
@@ -36,6 +36,8 @@ def main():
     ap.add_argument("--q", type=int, required=True)
     ap.add_argument("--m", type=int, required=True)
     ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--schedule", type=int, default=None,
+                    help="run this tlibttm_schedule id (tlibttm_ttm_sched) instead of the planner's choice")
     a = ap.parse_args()
     na = [int(x) for x in a.na.split(",")]
     pia = [int(x) for x in a.pia.split(",")] if a.pia else list(range(1, len(na) + 1))
@@ -55,8 +57,16 @@ def main():
     prec = _lib.PRECISIONS[a.precision]
 
     def run():
-        _lib.ttm_raw(dt, prec, q, len(na), A.data_ptr(), na, _dense(na, pia), pia, B.data_ptr(), [m, na[q - 1]],
-                     [1, 2], C.data_ptr(), nc, _dense(nc, pia), stream)
+        if a.schedule is None:
+            _lib.ttm_raw(dt, prec, q, len(na), A.data_ptr(), na, _dense(na, pia), pia, B.data_ptr(), [m, na[q - 1]],
+                         [1, 2], C.data_ptr(), nc, _dense(nc, pia), stream)
+            return
+        import ctypes as C_
+        from ttm_b200.selector import lib as sched_lib
+        _lib.check(sched_lib().tlibttm_ttm_sched(dt, a.schedule, q, len(na), C_.c_void_p(A.data_ptr()), _lib.sz(na),
+                                                 _lib.sz(_dense(na, pia)), _lib.sz(pia), C_.c_void_p(B.data_ptr()),
+                                                 _lib.sz([m, na[q - 1]]), _lib.sz([1, 2]), C_.c_void_p(C.data_ptr()),
+                                                 _lib.sz(nc), _lib.sz(_dense(nc, pia)), C_.c_void_p(stream)))
 
     run()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -1,7 +1,8 @@
 """Failure detection without a GPU fault (host-side injection through tlibttm_inject).
 
-* A bounded wait that runs out: the bf16x3 kernel's B producer never fills its first stage and
-  every mbarrier wait is bounded at 1 ms, so the MMA issuer's wait expires. The kernel's blocks
+* A bounded wait that runs out: the bf16x3 kernel's first pipeline stage is never filled (the
+  single-SM kernel's B stage; the pair kernel's first A stage in the even CTA) and every mbarrier
+  wait is bounded at 1 ms, so the waits on that stage expire. The kernel's blocks
   stop, drain their own copies, free tensor memory and raise the device status word;
   tlibttm_synchronize reports TLIBTTM_ERR_DEVICE once (the word is read and cleared), and the
   next call on the same context succeeds with correct results. The same for the allocation-free
@@ -62,12 +63,13 @@ def _want(a, b, md, q):
 
 
 @pytest.mark.parametrize("entry", ["ex", "noalloc"])
-def test_bounded_wait_runs_out_and_is_reported_once(cuda, entry):
+@pytest.mark.parametrize("m", [64, 256])   # the single-SM kernel, and the pair kernel (clusters of two)
+def test_bounded_wait_runs_out_and_is_reported_once(cuda, entry, m):
     import torch
     L = _lib.lib()
     stream = torch.cuda.current_stream().cuda_stream
     q, pia = 2, [1, 2, 3]
-    a, b, c, md = _problem(cuda, [256, 64, 40], pia, q, 64)
+    a, b, c, md = _problem(cuda, [256, 64, 40], pia, q, m)
 
     def call():
         args = _args(q, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream)
@@ -80,7 +82,7 @@ def test_bounded_wait_runs_out_and_is_reported_once(cuda, entry):
     _lib.inject(_lib.INJECT_WAIT_NS, SHORT_WAIT_NS)
     _lib.inject(_lib.INJECT_SKIP_B_STAGE, 1)
     assert call() == 0, L.tlibttm_last_error()            # the launch itself succeeds
-    assert _lib.last_kernel() == "tc_bf16x3"
+    assert _lib.last_kernel() == ("tc_bf16x3" if m <= 128 else "tc_bf16x3_pair")
     rc = L.tlibttm_synchronize(C.c_void_p(stream))
     assert rc == _lib.ERR_DEVICE, (rc, L.tlibttm_last_error())
     assert b"bounded wait" in L.tlibttm_last_error()

@@ -63,7 +63,7 @@ def test_noalloc_matches_existing_entry_point_twice(cuda):
         assert rc == 0, L.tlibttm_last_error()
         rc = _call("tlibttm_ttm_f32_bf16x3_noalloc", q, a.data_ptr(), b.data_ptr(), c_new.data_ptr(), md, stream)
         assert rc == 0, L.tlibttm_last_error()
-        assert _lib.last_kernel() == "tc_bf16x3"
+        assert _lib.last_kernel().startswith("tc_bf16x3")
         assert L.tlibttm_synchronize(C.c_void_p(stream)) == 0, L.tlibttm_last_error()
         x = c_new.double().cpu().numpy()
         y = c_old.double().cpu().numpy()
@@ -111,7 +111,8 @@ def test_noalloc_allocates_nothing(cuda):
     import torch
     L = _lib.lib()
     stream = torch.cuda.current_stream().cuda_stream
-    a, b, md = _problem(cuda, [256, 64, 40], [1, 2, 3], 2, 256, True, 6)
+    # m = 64: the single-SM kernel, whose B image the allocating entry point takes from the pool
+    a, b, md = _problem(cuda, [256, 64, 40], [1, 2, 3], 2, 64, True, 6)
     c = torch.empty(int(np.prod(md["nc"])), device=cuda)
     # first call on this device (its one-time symbol lookup) outside the measured window
     assert _call("tlibttm_ttm_f32_bf16x3_noalloc", 2, a.data_ptr(), b.data_ptr(), c.data_ptr(), md, stream) == 0

@@ -38,6 +38,7 @@ const char* kernel_name(int id)
     case K_GROUPED: return "grouped";
     case K_STREAM_COLS: return "stream_cols";
     case K_STREAM_ROWS: return "stream_rows";
+    case K_TC_PAIR: return "tc_bf16x3_pair";
     default: return "";
     }
 }
@@ -280,7 +281,7 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s, int64_t s
     if (precision != TLIBTTM_PREC_PLAIN && tc_supported(v, precision)) {
         int kid = K_NONE;
         cudaError_t e = launch_tc(v, precision, s, &kid);
-        if (e == cudaSuccess) ++g_launches;   // the operand-split kernel that precedes it
+        if (e == cudaSuccess && kid == K_TC_BF16X3) ++g_launches;   // the operand-split kernel that precedes it
         return note_launch(e, kid);
     }
     return note_launch(launch_simt_gemm(v, x.dtype, s), K_SIMT_GEMM);
@@ -589,7 +590,8 @@ int launches_of(const Single& sg, int dtype, int precision)
     if (pr == TLIBTTM_PREC_AUTO)
         pr = (dtype == TLIBTTM_F32 && tc_supported(sg.pl.v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3 : TLIBTTM_PREC_PLAIN;
     if (pr == TLIBTTM_PREC_FP8 || pr == TLIBTTM_PREC_OZAKI) return tc8_launches(sg.pl.v, pr);
-    return (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) ? 2 : 1;
+    if (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) return tc_pair_supported(sg.pl.v) ? 1 : 2;
+    return 1;
 }
 
 }  // namespace
@@ -731,6 +733,7 @@ static bool sched_valid_view(int dtype, int schedule, const View3& v)
     case TLIBTTM_SCHED_ROWS: return v.m <= kSmallM && v.inner == 1;
     case TLIBTTM_SCHED_TC_BF16X3: return dtype == TLIBTTM_F32 && tc_supported(v, TLIBTTM_PREC_BF16X3);
     case TLIBTTM_SCHED_COLS_TMA: return stream_supported(v, dtype);
+    case TLIBTTM_SCHED_TC_BF16X3_PAIR: return dtype == TLIBTTM_F32 && tc_pair_supported(v);
     default: return false;
     }
 }
@@ -769,9 +772,14 @@ int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p, const voi
     case TLIBTTM_SCHED_ROWS: return note_launch(launch_rowdot(v, dtype, s), K_ROWDOT);
     case TLIBTTM_SCHED_COLS_TMA:
         return note_launch(launch_stream(v, dtype, s), v.inner == 1 ? K_STREAM_ROWS : K_STREAM_COLS);
+    case TLIBTTM_SCHED_TC_BF16X3_PAIR: {
+        int* status = nullptr;
+        if ((e = tc_status_word(dev, &status)) != cudaSuccess) return cuda_fail(e, "tensor-core state");
+        return note_launch(launch_tc_pair(v, status, s), K_TC_PAIR);
+    }
     default: {
         int kid = K_NONE;
-        e = launch_tc(v, TLIBTTM_PREC_BF16X3, s, &kid);
+        e = launch_tc_single(v, s, &kid);
         if (e == cudaSuccess) ++g_launches;
         return note_launch(e, kid);
     }
@@ -834,7 +842,7 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
                                          "else ceil(m/256)*256; e.g. m = 256 with n_q <= 1024).");
     int kid = K_NONE;
     e = launch_tc_noalloc(v, static_cast<cudaStream_t>(stream), &kid);
-    if (e == cudaSuccess) ++g_launches;   // split_b_kernel; note_launch counts the main kernel
+    if (e == cudaSuccess && kid == K_TC_BF16X3) ++g_launches;   // split_b_kernel; note_launch counts the main kernel
     return note_launch(e, kid);
 }
 

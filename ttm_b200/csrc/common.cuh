@@ -91,6 +91,7 @@ enum KernelId : int {
     K_GROUPED,
     K_STREAM_COLS,
     K_STREAM_ROWS,
+    K_TC_PAIR,
     K_COUNT
 };
 
@@ -125,8 +126,8 @@ cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t s);
 
 // Bound of the bounded mbarrier waits of the bf16x3 kernel, in ns (4 s unless a test set it).
 unsigned long long wait_limit_ns();
-// True once after a test asked for it: the next bf16x3 launch's B producer skips its first
-// stage (no copy, no arrive), so that the MMA issuer's bounded wait runs out.
+// True once after a test asked for it: the next bf16x3 launch never fills its first pipeline
+// stage (no copy, no arrive), so that the bounded waits on that stage run out.
 bool take_skip_b();
 
 }  // namespace tlibttm

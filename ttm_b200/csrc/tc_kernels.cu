@@ -58,11 +58,13 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn_major)
            ((uint32_t)(kBM >> 4) << 24);
 }
 
+// Called by a whole converged warp with warp-uniform operands (so that they stay in uniform
+// registers); one elected lane issues the instruction.
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
 {
     asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        "{\n .reg .pred p, e;\n setp.ne.b32 p, %4, 0;\n elect.sync _|e, 0xffffffff;\n"
+        " @e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
         ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc)
         : "memory");
 }
@@ -294,7 +296,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------- MMA issuer
-        if (lane == 0) {
+        // The whole warp runs the loop (warp-uniform descriptors); one elected lane issues each
+        // MMA and commit; wait results are made warp-uniform before they steer the loop.
+        {
             const uint32_t idesc = idesc_bf16(P.nt, GEOM == GEOM_MN);
             // descriptors of stage 0's first sub-block; a descriptor's start-address field is
             // address / 16 in its low bits, so other stages and parts are plain additions
@@ -307,11 +311,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t cph = 0;
             bool ok = true;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                if (!mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag, P.wait_ns)) break;
+                if (!__all_sync(0xffffffffu, mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag, P.wait_ns))) break;
                 tc_fence_after();
                 const uint32_t dcol = tmem_base + (uint32_t)(ab * P.nt);
                 for (int st = 0; st < kstages; ++st) {
-                    if (!mbar_wait(&b_full[bs], bph, abort_flag, P.wait_ns) || !mbar_wait(&a_conv[as], aph, abort_flag, P.wait_ns)) {
+                    const bool got = mbar_wait(&b_full[bs], bph, abort_flag, P.wait_ns) &&
+                                     mbar_wait(&a_conv[as], aph, abort_flag, P.wait_ns);
+                    if (!__all_sync(0xffffffffu, got)) {
                         ok = false;
                         break;
                     }
@@ -328,19 +334,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                         mma_bf16(dcol, dahi, dblo, idesc, 1u);
                         mma_bf16(dcol, dalo, dbhi, idesc, 1u);
                     }
-                    mma_commit(&a_empty[as]);   // stages free once these MMAs have read them
-                    mma_commit(&b_empty[bs]);
+                    mma_commit_warp(&a_empty[as]);   // stages free once these MMAs have read them
+                    mma_commit_warp(&b_empty[bs]);
                     if (++as == AS) { as = 0; aph ^= 1; }
                     if (++bs == BS) { bs = 0; bph ^= 1; }
                 }
                 if (!ok) break;
-                mma_commit(&acc_full[ab]);     // accumulator ready for the epilogue
+                mma_commit_warp(&acc_full[ab]);     // accumulator ready for the epilogue
                 if (++ab == 2) { ab = 0; cph ^= 1; }
             }
             // No MMA of this CTA may still be writing TMEM when it is freed.
-            mma_commit(drain);
+            mma_commit_warp(drain);
             const unsigned long long t0 = gtimer();
             while (!mbar_try(drain, 0) && gtimer() - t0 < kTimeoutNs) {}
+            __syncwarp();
         }
     } else if (warp < 3 + kConvWarps) {
         // ------------------------------------------------------------- converters (in place)
@@ -1492,6 +1499,21 @@ cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid)
 {
     *kid = K_TC_BF16X3;
     if (precision != TLIBTTM_PREC_BF16X3) return cudaErrorNotSupported;
+    if (tc_pair_supported(v)) {
+        *kid = K_TC_PAIR;
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        DevState* st = nullptr;
+        if ((e = state_for(dev, st)) != cudaSuccess) return e;
+        return launch_tc_pair(v, st->status, s);
+    }
+    return launch_tc_single(v, s, kid);
+}
+
+cudaError_t launch_tc_single(const View3& v, cudaStream_t s, int* kid)
+{
+    *kid = K_TC_BF16X3;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -1564,12 +1586,18 @@ size_t tc_image_bytes(const View3& v)
 cudaError_t launch_tc_noalloc(const View3& v, cudaStream_t s, int* kid)
 {
     *kid = K_TC_BF16X3;
-    if (tc_image_bytes(v) > kNoAllocImageBytes) return cudaErrorInvalidValue;
+    if (!tc_pair_supported(v) && tc_image_bytes(v) > kNoAllocImageBytes) return cudaErrorInvalidValue;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     NoAllocSymbols sy;
     if ((e = noalloc_symbols(dev, sy)) != cudaSuccess) return e;
+    if (tc_pair_supported(v)) {
+        // the pair kernel keeps B in tensor memory: no image, only the status word
+        *kid = K_TC_PAIR;
+        if ((e = cudaMemsetAsync(sy.status, 0, sizeof(int), s)) != cudaSuccess) return e;
+        return launch_tc_pair(v, sy.status, s);
+    }
     int sms = 0;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(sy.status, 0, sizeof(int), s)) != cudaSuccess) return e;

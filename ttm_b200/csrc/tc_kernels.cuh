@@ -9,8 +9,18 @@ namespace tlibttm {
 bool tc_supported(const View3& v, int precision);
 
 // Launches the tensor-core path of `precision` on stream s; *kid receives the
-// identifier of the main kernel launched.
+// identifier of the main kernel launched: K_TC_PAIR (one launch) where tc_pair_supported,
+// else K_TC_BF16X3 (the operand-split kernel and the single-SM kernel).
 cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid);
+
+// The single-SM bf16x3 kernel (and its operand split) whatever the shape.
+cudaError_t launch_tc_single(const View3& v, cudaStream_t s, int* kid);
+
+// bf16x3 on pairs of SMs with B resident in tensor memory (tc_pair.cu): float, 128 < m <= 256,
+// n_q <= 256, A 16-byte aligned, and either contiguous fibres with n_q % 4 == 0 or inner >= 128
+// with inner % 4 == 0. Allocates nothing; `status` is the device status word it raises.
+bool tc_pair_supported(const View3& v);
+cudaError_t launch_tc_pair(const View3& v, int* status, cudaStream_t s);
 
 // Creates the per-device state of the tensor-core paths ahead of time (so that a later stream
 // capture does not need to allocate it).

@@ -117,6 +117,16 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar)
                  : "memory");
 }
 
+// mma_commit for a whole converged warp: one elected lane (the lowest, the same lane that
+// issued the MMAs through elect.sync) commits.
+__device__ __forceinline__ void mma_commit_warp(uint64_t* bar)
+{
+    asm volatile("{\n .reg .pred e;\n elect.sync _|e, 0xffffffff;\n"
+                 " @e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n}\n"
+                 ::"r"(su32(bar))
+                 : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
 {
     asm volatile(
