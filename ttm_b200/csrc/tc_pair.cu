@@ -343,9 +343,9 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                 uint32_t off[kIt];
 #pragma unroll
                 for (int it = 0; it < kIt; ++it) {
-                    const int v = gt + kGroupWarpsP * 32 * it;   // float4 index within the 8 KB stage
+                    const int v = gt + kGroupWarpsP * 32 * it;   // float4 index within the stage
                     if (GEOM == PGEOM_MN) {
-                        const int l = v >> 4, w = v & 15;          // [32 l][64 i], 256-byte rows
+                        const int l = v >> 4, w = v & 15;          // [16 kPSub l][64 i], 256-byte rows
                         if (have) x[it] = *reinterpret_cast<const float4*>(buf + l * 256 + w * 16);
                         off[it] = (uint32_t)(l >> 4) * kSubBytes + mn64_off((uint32_t)(l & 15), (uint32_t)(w >> 1));
                     } else {

@@ -2,7 +2,8 @@
 
 A *schedule* is one of the planner's kernel choices (include/tlibttm.h, tlibttm_schedule):
 SIMT slice-GEMM, the two small-m kernels for strided fibres, the small-m kernel for contiguous
-fibres, and the bf16x3 tensor-core kernel. The autotuner times every schedule valid for a
+fibres, the TMA-fed small-m kernel, and the two bf16x3 tensor-core kernels (single SMs, and
+pairs of SMs with B in tensor memory). The autotuner times every schedule valid for a
 problem (CUDA events, median of a few runs) and keeps the results in a timing database. The
 selector is a small multilayer perceptron (3 hidden layers of 64, ReLU) that predicts each
 schedule's log2 run time from the problem's shape (p, q, log2 extents, layout, m, dtype); it is
@@ -33,7 +34,7 @@ try:
 except Exception:  # noqa: BLE001
     torch = None
 
-SCHEDULES = ["simt_gemm", "cols", "cols_split", "rows", "tc_bf16x3", "cols_tma"]   # ids 1..6 of tlibttm_schedule
+SCHEDULES = ["simt_gemm", "cols", "cols_split", "rows", "tc_bf16x3", "cols_tma", "tc_bf16x3_pair"]   # ids 1..7
 EXACT = [1, 2, 3, 4, 6]               # schedules that compute with exact FMA in the I/O type
 NS = len(SCHEDULES)
 FEATURES = 53
@@ -394,7 +395,10 @@ def _heuristic_in(pr, allowed):
         rv = 16 // es
         w = rv if inner % rv == 0 else 1
         return 3 if math.ceil(inner * outer / (32 * w)) < 148 * 32 else 2
-    if 5 in allowed and valid_mask(pr)[4]:
+    ok = valid_mask(pr)
+    if 7 in allowed and ok[6]:
+        return 7
+    if 5 in allowed and ok[4]:
         return 5
     return 1
 
