@@ -39,6 +39,7 @@ const char* kernel_name(int id)
     case K_STREAM_COLS: return "stream_cols";
     case K_STREAM_ROWS: return "stream_rows";
     case K_TC_PAIR: return "tc_bf16x3_pair";
+    case K_BVEC: return "bvec";
     default: return "";
     }
 }
@@ -278,13 +279,32 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s, int64_t s
         if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);   // exponent and slicer kernels
         return note_launch(e, kid);
     }
-    if (precision != TLIBTTM_PREC_PLAIN && tc_supported(v, precision)) {
-        int kid = K_NONE;
-        cudaError_t e = launch_tc(v, precision, s, &kid);
-        if (e == cudaSuccess && kid == K_TC_BF16X3) ++g_launches;   // the operand-split kernel that precedes it
-        return note_launch(e, kid);
+    // Few output rows and a long l range: stream B over the whole GPU (exact FMA; these shapes are
+    // bound by reading B, so a split into bf16 parts would gain nothing).
+    if (bvec_supported(v)) {
+        int n = 1;
+        cudaError_t e = launch_bvec(v, x.dtype, s, &n);
+        if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);
+        return note_launch(e, K_BVEC);
     }
-    return note_launch(launch_simt_gemm(v, x.dtype, s), K_SIMT_GEMM);
+    if (precision != TLIBTTM_PREC_PLAIN && tc_supported(v, precision)) {
+        // The single-SM tensor-core kernel has no K split: when its tiles fill less than half the
+        // GPU and the l range is long, the split-K SIMT GEMM (exact) is the faster choice.
+        int sms = 0;
+        const bool few = !tc_pair_supported(v) && v.nq >= 2048 &&
+                         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0) == cudaSuccess &&
+                         tc_single_tiles(v) * 2 < sms;
+        if (!few) {
+            int kid = K_NONE;
+            cudaError_t e = launch_tc(v, precision, s, &kid);
+            if (e == cudaSuccess && kid == K_TC_BF16X3) ++g_launches;   // the operand-split kernel that precedes it
+            return note_launch(e, kid);
+        }
+    }
+    int n = 1;
+    cudaError_t e = launch_simt_gemm(v, x.dtype, s, &n);
+    if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);   // the reduction of a split K loop
+    return note_launch(e, K_SIMT_GEMM);
 }
 
 // ---- staging of host operands ---------------------------------------------------------------
@@ -590,8 +610,15 @@ int launches_of(const Single& sg, int dtype, int precision)
     if (pr == TLIBTTM_PREC_AUTO)
         pr = (dtype == TLIBTTM_F32 && tc_supported(sg.pl.v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3 : TLIBTTM_PREC_PLAIN;
     if (pr == TLIBTTM_PREC_FP8 || pr == TLIBTTM_PREC_OZAKI) return tc8_launches(sg.pl.v, pr);
-    if (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) return tc_pair_supported(sg.pl.v) ? 1 : 2;
-    return 1;
+    if (bvec_supported(sg.pl.v)) return 2;
+    if (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) {
+        int sms = 0;
+        const bool few = !tc_pair_supported(sg.pl.v) && sg.pl.v.nq >= 2048 &&
+                         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0) == cudaSuccess &&
+                         tc_single_tiles(sg.pl.v) * 2 < sms;
+        if (!few) return tc_pair_supported(sg.pl.v) ? 1 : 2;
+    }
+    return simt_gemm_launch_count(sg.pl.v, dtype);
 }
 
 }  // namespace
@@ -766,7 +793,12 @@ int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p, const voi
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     switch (schedule) {
     case TLIBTTM_SCHED_HEURISTIC: return run_device(x, pl, TLIBTTM_PREC_PLAIN, s);
-    case TLIBTTM_SCHED_SIMT_GEMM: return note_launch(launch_simt_gemm(v, dtype, s), K_SIMT_GEMM);
+    case TLIBTTM_SCHED_SIMT_GEMM: {
+        int n = 1;
+        e = launch_simt_gemm(v, dtype, s, &n);
+        if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);
+        return note_launch(e, K_SIMT_GEMM);
+    }
     case TLIBTTM_SCHED_COLS: return note_launch(launch_colvec_ls(v, dtype, 1, s), K_COLVEC);
     case TLIBTTM_SCHED_COLS_SPLIT: return note_launch(launch_colvec_ls(v, dtype, 8, s), K_COLVEC);
     case TLIBTTM_SCHED_ROWS: return note_launch(launch_rowdot(v, dtype, s), K_ROWDOT);

@@ -92,13 +92,21 @@ enum KernelId : int {
     K_STREAM_COLS,
     K_STREAM_ROWS,
     K_TC_PAIR,
+    K_BVEC,
     K_COUNT
 };
 
 const char* kernel_name(int id);
 
 // Launchers (simt_kernels.cu). Return cudaSuccess or the launch error.
-cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s);
+// The slice-GEMM; when its tiles cannot fill the GPU and n_q is long, the K loop is split over
+// more blocks and the parts are added by a second kernel (*launches = 2, else 1).
+cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s, int* launches = nullptr);
+int simt_gemm_launch_count(const View3& v, int dtype);
+// Few output rows (outer * inner <= 8), 16 < m <= 256, n_q >= 4096: a kernel that streams B with
+// the l range split over the GPU, then a fixed-order reduction (*launches = 2).
+bool bvec_supported(const View3& v);
+cudaError_t launch_bvec(const View3& v, int dtype, cudaStream_t s, int* launches = nullptr);
 cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s);
 // colvec with an explicit l split over warps (1 or 8).
 cudaError_t launch_colvec_ls(const View3& v, int dtype, int ls, cudaStream_t s);

@@ -76,7 +76,8 @@ struct GemmSmem {
 
 // One BM x BN output tile (rows m0.., columns n0..) of the slice-GEMM, all 256 threads of the block.
 template <typename T, bool AK, bool VEC, bool BCM>
-__device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0, GemmSmem<T>& sm)
+__device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0, GemmSmem<T>& sm,
+                                          int64_t l_begin = 0, int64_t l_end = -1)
 {
     constexpr int RV = 16 / sizeof(T);   // elements per 16-byte vector
     constexpr int BM = 32 * RV, BN = 32 * RV, BK = 8;
@@ -96,7 +97,10 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
     const T* __restrict__ A = static_cast<const T*>(v.a);
     const T* __restrict__ B = static_cast<const T*>(v.b);
     T* __restrict__ Cp = static_cast<T*>(v.c);
-    const int64_t inner = v.inner, nq = v.nq, m = v.m;
+    const int64_t inner = v.inner, m = v.m;
+    // the l range of this tile: all of n_q, or one part of a split K loop (l_begin % BK == 0)
+    const int64_t nq = l_end < 0 ? v.nq : l_end;
+    const int64_t nq_full = v.nq;
     const int64_t M = v.outer * inner;
     const int tid = threadIdx.x;
     const int tx = tid % 16, ty = tid / 16;
@@ -116,7 +120,7 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
         arow_ok[s] = row < M;
         const int64_t k = arow_ok[s] ? row / inner : 0;
         const int64_t i = arow_ok[s] ? row - k * inner : 0;
-        abase[s] = k * inner * nq + i;
+        abase[s] = k * inner * nq_full + i;
         a_loff[s] = loff;
         a_roff[s] = roff;
     }
@@ -143,7 +147,7 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
             else     { lo = vi % BK; jo = vi / BK; }
             const int64_t j = n0 + jo, l = l0 + lo;
             T val = T(0);
-            if (j < m && l < nq) val = __ldg(BCM ? B + j + l * m : B + j * nq + l);
+            if (j < m && l < nq) val = __ldg(BCM ? B + j + l * m : B + j * nq_full + l);
             rb[s] = val;
         }
     };
@@ -182,14 +186,14 @@ __device__ __forceinline__ void gemm_tile(const View3& v, int64_t m0, int64_t n0
             for (int j = 0; j < TN / 2; ++j) acc2[i][j] = 0ull;
     }
 
-    const int64_t nk = ceil_div(nq, BK);
-    load_tiles(0);
+    const int64_t nk = ceil_div(nq - l_begin, BK);
+    load_tiles(l_begin);
     store_tiles(0);
     __syncthreads();
 
     for (int64_t kt = 0; kt < nk; ++kt) {
         const int buf = kt & 1;
-        if (kt + 1 < nk) load_tiles((kt + 1) * BK);
+        if (kt + 1 < nk) load_tiles(l_begin + (kt + 1) * BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
             if constexpr (PK) {
@@ -307,6 +311,22 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 3 : 2)) simt_gemm_kerne
     constexpr int RV = 16 / sizeof(T);
     __shared__ GemmSmem<T> sm;
     gemm_tile<T, AK, VEC, BCM>(v, (int64_t)blockIdx.x * (32 * RV), (int64_t)blockIdx.y * (32 * RV), sm);
+}
+
+// The K loop split `gridDim.z` ways: part z covers l in [z * lper, min(n_q, (z + 1) * lper)) and
+// writes its partial tile into ws + z * (outer * m * inner), a buffer with C's own layout;
+// split_reduce_kernel then adds the parts in a fixed order, so the result does not depend on
+// scheduling.
+template <typename T, bool AK, bool VEC, bool BCM>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 3 : 2)) simt_gemm_split_kernel(View3 v, int64_t lper, T* ws)
+{
+    constexpr int RV = 16 / sizeof(T);
+    __shared__ GemmSmem<T> sm;
+    const int64_t l0 = (int64_t)blockIdx.z * lper;
+    const int64_t l1 = l0 + lper < v.nq ? l0 + lper : v.nq;
+    View3 part = v;
+    part.c = ws + (size_t)blockIdx.z * (size_t)(v.outer * v.m * v.inner);
+    gemm_tile<T, AK, VEC, BCM>(part, (int64_t)blockIdx.x * (32 * RV), (int64_t)blockIdx.y * (32 * RV), sm, l0, l1);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -802,18 +822,22 @@ __global__ void __launch_bounds__(256, 2) grouped_kernel(const GroupDesc* __rest
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 template <typename T>
-cudaError_t simt_gemm_dispatch(const View3& v, cudaStream_t s)
+cudaError_t simt_gemm_dispatch(const View3& v, cudaStream_t s, int split = 1, int64_t lper = 0, T* ws = nullptr)
 {
     constexpr int RV = 16 / sizeof(T);
     constexpr int BM = 32 * RV, BN = 32 * RV;
     const bool ak = v.inner == 1;
-    bool vec = aligned16(v.a) && aligned16(v.c);
+    bool vec = aligned16(v.a) && aligned16(split > 1 ? static_cast<const void*>(ws) : v.c);
     if (ak) vec = vec && (v.nq % RV == 0) && (v.m % RV == 0);
     else vec = vec && (v.inner % RV == 0);
     const int64_t M = v.outer * v.inner;
-    dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(v.m, BN));
+    dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(v.m, BN), (unsigned)split);
     dim3 block(256);
-#define TLIBTTM_GEMM(AKv, VECv, BCMv) simt_gemm_kernel<T, AKv, VECv, BCMv><<<grid, block, 0, s>>>(v)
+#define TLIBTTM_GEMM(AKv, VECv, BCMv)                                                            \
+    do {                                                                                        \
+        if (split > 1) simt_gemm_split_kernel<T, AKv, VECv, BCMv><<<grid, block, 0, s>>>(v, lper, ws); \
+        else simt_gemm_kernel<T, AKv, VECv, BCMv><<<grid, block, 0, s>>>(v);                     \
+    } while (0)
     if (ak) {
         if (vec) { if (v.b_cm) TLIBTTM_GEMM(true, true, true); else TLIBTTM_GEMM(true, true, false); }
         else     { if (v.b_cm) TLIBTTM_GEMM(true, false, true); else TLIBTTM_GEMM(true, false, false); }
@@ -940,11 +964,311 @@ cudaError_t rowdot_dispatch(const View3& v, cudaStream_t s)
     return vec ? rowdot_dispatch_v<T, true>(v, s) : rowdot_dispatch_v<T, false>(v, s);
 }
 
+// Sum of the `parts` partial results of a split K loop, in a fixed order: c[i] = sum_z ws[z][i].
+template <typename T>
+__global__ void __launch_bounds__(256) split_reduce_kernel(const T* __restrict__ ws, int parts, int64_t n, T* __restrict__ c)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        T sum = ws[i];
+        for (int z = 1; z < parts; ++z) sum += ws[(size_t)z * n + i];
+        c[i] = sum;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// bvec: few output rows (R = outer * inner <= 8) and m <= 256: C[r][j] = sum_l A[r][l] B(j,l),
+// bound by reading B (m x n_q), e.g. the order-1 product c = B a. Block b of G streams the
+// contiguous l range [b lper, (b + 1) lper) of B; its partial C goes to ws[b][r][j] and
+// bvec_reduce_kernel adds the G partials in a fixed order.
+//   column-major B (B(j,l) = b[j + l m], the range is one contiguous block of B): thread =
+//     (j vector jv of W consecutive j, l lane ls of LS); a warp's loads for one l are
+//     consecutive; the LS lane partials are added in lane order at the end;
+//   row-major B (B(j,l) = b[j n_q + l]): the range is cut into tiles of kBvecTile l; warp w owns
+//     rows j = w, w + 8, ... and reads W consecutive l per lane (A's tile stays in L1 across the
+//     rows); warp shuffles reduce, and the warp alone adds into its rows' shared partials.
+// W = 16 / sizeof(T) when the vector accesses are aligned (VEC), else 1.
+// ---------------------------------------------------------------------------------------------
+constexpr int kBvecMaxR = 8, kBvecMaxM = 256, kBvecTile = 1024;
+
+template <typename T, int R>
+__device__ __forceinline__ T bvec_a(const T* __restrict__ A, const View3& v, int r, int64_t l)
+{
+    const int64_t k = r / v.inner, i = r - k * v.inner;
+    return __ldg(A + (k * v.nq + l) * v.inner + i);
+}
+
+template <typename T, int R, bool VEC>
+__global__ void __launch_bounds__(256) bvec_cm_kernel(View3 v, int64_t lper, T* __restrict__ ws)
+{
+    constexpr int W = VEC ? 16 / (int)sizeof(T) : 1;
+    extern __shared__ __align__(16) uint8_t bvec_smem[];
+    T* red = reinterpret_cast<T*>(bvec_smem);                 // [LS][R][m]
+    const T* __restrict__ A = static_cast<const T*>(v.a);
+    const T* __restrict__ B = static_cast<const T*>(v.b);
+    const int64_t m = v.m;
+    const int JV = (int)((m + W - 1) / W), LS = 256 / JV;
+    const int tid = threadIdx.x, jv = tid % JV, ls = tid / JV;
+    const int64_t l0 = (int64_t)blockIdx.x * lper, l1 = l0 + lper < v.nq ? l0 + lper : v.nq;
+    const int Rv = (int)(v.outer * v.inner);
+    T acc[W][R];
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+#pragma unroll
+        for (int r = 0; r < R; ++r) acc[w][r] = T(0);
+    if (ls < LS) {
+#pragma unroll 4
+        for (int64_t l = l0 + ls; l < l1; l += LS) {
+            T a[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[r] = r < Rv ? bvec_a<T, R>(A, v, r, l) : T(0);
+            T b[W];
+            const T* bp = B + l * m + (int64_t)jv * W;
+            if constexpr (VEC) {
+                typedef typename V16<T>::type VT;
+                const VT x = __ldg(reinterpret_cast<const VT*>(bp));
+#pragma unroll
+                for (int w = 0; w < W; ++w) b[w] = reinterpret_cast<const T*>(&x)[w];
+            } else {
+                b[0] = __ldg(bp);
+            }
+#pragma unroll
+            for (int w = 0; w < W; ++w)
+#pragma unroll
+                for (int r = 0; r < R; ++r) acc[w][r] = fma_t(a[r], b[w], acc[w][r]);
+        }
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const int64_t j = (int64_t)jv * W + w;
+            if (j < m) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) red[((size_t)ls * R + r) * m + j] = acc[w][r];
+            }
+        }
+    }
+    __syncthreads();
+    T* wb = ws + (size_t)blockIdx.x * (size_t)(R * m);
+    for (int e = tid; e < R * m; e += 256) {
+        T sum = red[e];
+        for (int q = 1; q < LS; ++q) sum += red[(size_t)q * R * m + e];
+        wb[e] = sum;
+    }
+}
+
+template <typename T, int R, bool VEC>
+__global__ void __launch_bounds__(256) bvec_rm_kernel(View3 v, int64_t lper, T* __restrict__ ws)
+{
+    constexpr int W = VEC ? 16 / (int)sizeof(T) : 1;
+    __shared__ T part[R][kBvecMaxM];
+    const T* __restrict__ A = static_cast<const T*>(v.a);
+    const T* __restrict__ B = static_cast<const T*>(v.b);
+    const int64_t m = v.m, nq = v.nq;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t l0 = (int64_t)blockIdx.x * lper, l1 = l0 + lper < nq ? l0 + lper : nq;
+    const int Rv = (int)(v.outer * v.inner);
+    for (int e = tid; e < R * kBvecMaxM; e += 256) part[e / kBvecMaxM][e % kBvecMaxM] = T(0);
+    __syncthreads();
+    for (int64_t t0 = l0; t0 < l1; t0 += kBvecTile) {
+        const int64_t t1 = t0 + kBvecTile < l1 ? t0 + kBvecTile : l1;
+        for (int64_t j = warp; j < m; j += 8) {
+            const T* bj = B + j * nq;
+            T acc[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = T(0);
+#pragma unroll 2
+            for (int64_t l = t0 + (int64_t)lane * W; l < t1; l += 32 * W) {
+                T b[W], a[W][R];
+                if constexpr (VEC) {
+                    typedef typename V16<T>::type VT;
+                    const VT x = __ldg(reinterpret_cast<const VT*>(bj + l));
+#pragma unroll
+                    for (int w = 0; w < W; ++w) b[w] = reinterpret_cast<const T*>(&x)[w];
+                    if constexpr (R == 1) {
+                        // one row, inner == 1 (VEC requires it for R == 1): A's W values in one load
+                        const VT y = __ldg(reinterpret_cast<const VT*>(A + l));
+#pragma unroll
+                        for (int w = 0; w < W; ++w) a[w][0] = reinterpret_cast<const T*>(&y)[w];
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < W; ++w)
+#pragma unroll
+                            for (int r = 0; r < R; ++r) a[w][r] = r < Rv ? bvec_a<T, R>(A, v, r, l + w) : T(0);
+                    }
+                } else {
+                    b[0] = __ldg(bj + l);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) a[0][r] = r < Rv ? bvec_a<T, R>(A, v, r, l) : T(0);
+                }
+#pragma unroll
+                for (int w = 0; w < W; ++w)
+#pragma unroll
+                    for (int r = 0; r < R; ++r) acc[r] = fma_t(a[w][r], b[w], acc[r]);
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[r] += __shfl_xor_sync(0xffffffffu, acc[r], o);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) part[r][j] += acc[r];
+            }
+        }
+    }
+    __syncthreads();
+    T* wb = ws + (size_t)blockIdx.x * (size_t)(R * m);
+    for (int e = tid; e < R * m; e += 256) wb[e] = part[e / m][e % m];
+}
+
+// ws[g][r][j] -> C[k][j][i] (r = k inner + i): sum over the G block partials in block order.
+template <typename T>
+__global__ void __launch_bounds__(256) bvec_reduce_kernel(const T* __restrict__ ws, int G, View3 v, int R)
+{
+    T* C = static_cast<T*>(v.c);
+    const int64_t n = (int64_t)R * v.m;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / v.m, j = e - r * v.m;
+        if (r >= v.outer * v.inner) continue;
+        T sum = T(0);
+        for (int g = 0; g < G; ++g) sum += ws[(size_t)g * n + e];
+        const int64_t k = r / v.inner, i = r - k * v.inner;
+        C[(k * v.m + j) * v.inner + i] = sum;
+    }
+}
+
+template <typename T, int R>
+cudaError_t bvec_launch_r(const View3& v, int G, int64_t lper, bool vec, T* ws, cudaStream_t s)
+{
+    if (v.b_cm) {
+        constexpr int WV = 16 / (int)sizeof(T);
+        const int W = vec ? WV : 1;
+        const int JV = (int)((v.m + W - 1) / W), LS = 256 / JV;
+        const size_t smem = (size_t)LS * R * v.m * sizeof(T);
+        if (vec) bvec_cm_kernel<T, R, true><<<G, 256, smem, s>>>(v, lper, ws);
+        else bvec_cm_kernel<T, R, false><<<G, 256, smem, s>>>(v, lper, ws);
+    } else {
+        if (vec) bvec_rm_kernel<T, R, true><<<G, 256, 0, s>>>(v, lper, ws);
+        else bvec_rm_kernel<T, R, false><<<G, 256, 0, s>>>(v, lper, ws);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t bvec_dispatch(const View3& v, int sms, cudaStream_t s, int* launches)
+{
+    constexpr int WV = 16 / (int)sizeof(T);
+    const int64_t R = v.outer * v.inner;
+    const int Rt = R <= 1 ? 1 : R <= 2 ? 2 : R <= 4 ? 4 : 8;
+    // 16-byte accesses: B's j vectors (column-major) or l vectors (row-major; for one row also A's)
+    bool vec = aligned16(v.b) && (v.b_cm ? v.m % WV == 0 : v.nq % WV == 0);
+    if (!v.b_cm && Rt == 1) vec = vec && v.inner == 1 && aligned16(v.a);
+    // contiguous l ranges of at least 4096 l, eight blocks per SM at most; starts on vector boundaries
+    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(v.nq, 4096), (int64_t)sms * 8));
+    const int64_t lper = ceil_div(ceil_div(v.nq, G), WV) * WV;
+    const int Gr = (int)ceil_div(v.nq, lper);
+    T* ws = nullptr;
+    cudaError_t e = dev_malloc_async(reinterpret_cast<void**>(&ws), (size_t)Gr * Rt * v.m * sizeof(T), s);
+    if (e != cudaSuccess) return e;
+    switch (Rt) {
+    case 1: e = bvec_launch_r<T, 1>(v, Gr, lper, vec, ws, s); break;
+    case 2: e = bvec_launch_r<T, 2>(v, Gr, lper, vec, ws, s); break;
+    case 4: e = bvec_launch_r<T, 4>(v, Gr, lper, vec, ws, s); break;
+    default: e = bvec_launch_r<T, 8>(v, Gr, lper, vec, ws, s); break;
+    }
+    if (e == cudaSuccess) {
+        const int64_t n = (int64_t)Rt * v.m;
+        bvec_reduce_kernel<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), 1024)), 256, 0, s>>>(
+            ws, Gr, v, Rt);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(ws, s);
+    if (launches) *launches = 2;
+    return e;
+}
+
+int g_sms_simt = 0;
+
+cudaError_t sms_of_device(int& sms)
+{
+    if (!g_sms_simt) {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&g_sms_simt, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+    }
+    sms = g_sms_simt;
+    return cudaSuccess;
+}
+
+// Parts of the K loop for a slice-GEMM whose tiles cannot fill the GPU (1 when none is needed).
+template <typename T>
+int gemm_split_parts(const View3& v, int sms, int64_t& lper)
+{
+    constexpr int RV = 16 / sizeof(T);
+    constexpr int64_t BM = 32 * RV, BN = 32 * RV, BK = 8;
+    const int64_t tiles = ceil_div(v.outer * v.inner, BM) * ceil_div(v.m, BN);
+    const int64_t slots = (int64_t)sms * (sizeof(T) == 8 ? 3 : 2);
+    lper = v.nq;
+    if (tiles * 2 > slots || v.nq < 2048) return 1;
+    int64_t S = std::min<int64_t>(ceil_div(slots, tiles), v.nq / 1024);
+    S = std::min<int64_t>(S, 256);
+    // workspace of S partial results at most 1 GiB
+    const int64_t nc = v.outer * v.m * v.inner;
+    while (S > 1 && S * nc * (int64_t)sizeof(T) > (int64_t(1) << 30)) --S;
+    if (S <= 1) return 1;
+    lper = ceil_div(ceil_div(v.nq, S), BK) * BK;
+    return (int)ceil_div(v.nq, lper);
+}
+
+template <typename T>
+cudaError_t simt_gemm_launch(const View3& v, cudaStream_t s, int* launches)
+{
+    int sms = 0;
+    cudaError_t e = sms_of_device(sms);
+    if (e != cudaSuccess) return e;
+    int64_t lper = 0;
+    const int S = gemm_split_parts<T>(v, sms, lper);
+    if (launches) *launches = S > 1 ? 2 : 1;
+    if (S <= 1) return simt_gemm_dispatch<T>(v, s);
+    const int64_t nc = v.outer * v.m * v.inner;
+    T* ws = nullptr;
+    if ((e = dev_malloc_async(reinterpret_cast<void**>(&ws), (size_t)S * nc * sizeof(T), s)) != cudaSuccess) return e;
+    e = simt_gemm_dispatch<T>(v, s, S, lper, ws);
+    if (e == cudaSuccess) {
+        split_reduce_kernel<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nc, 256), 4096)), 256, 0, s>>>(
+            ws, S, nc, static_cast<T*>(v.c));
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(ws, s);
+    return e;
+}
+
 }  // namespace
 
-cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s)
+cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s, int* launches)
 {
-    return dtype == 0 ? simt_gemm_dispatch<float>(v, s) : simt_gemm_dispatch<double>(v, s);
+    return dtype == 0 ? simt_gemm_launch<float>(v, s, launches) : simt_gemm_launch<double>(v, s, launches);
+}
+
+int simt_gemm_launch_count(const View3& v, int dtype)
+{
+    int sms = 0;
+    if (sms_of_device(sms) != cudaSuccess) return 1;
+    int64_t lper = 0;
+    const int S = dtype == 0 ? gemm_split_parts<float>(v, sms, lper) : gemm_split_parts<double>(v, sms, lper);
+    return S > 1 ? 2 : 1;
+}
+
+bool bvec_supported(const View3& v)
+{
+    return v.m > kSmallM && v.m <= kBvecMaxM && v.outer * v.inner <= kBvecMaxR && v.nq >= 4096;
+}
+
+cudaError_t launch_bvec(const View3& v, int dtype, cudaStream_t s, int* launches)
+{
+    int sms = 0;
+    cudaError_t e = sms_of_device(sms);
+    if (e != cudaSuccess) return e;
+    return dtype == 0 ? bvec_dispatch<float>(v, sms, s, launches) : bvec_dispatch<double>(v, sms, s, launches);
 }
 
 cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s)

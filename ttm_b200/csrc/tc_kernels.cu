@@ -1511,6 +1511,17 @@ cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid)
     return launch_tc_single(v, s, kid);
 }
 
+int64_t tc_single_tiles(const View3& v)
+{
+    const int64_t nt = std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
+    const int64_t jblocks = (v.m + nt - 1) / nt;
+    int64_t tiles_m;
+    if (geometry_of(v) == GEOM_K) tiles_m = (v.outer + kBM - 1) / kBM;
+    else if (v.inner <= 64) tiles_m = (v.outer + (kBM >> (v.inner <= 32 ? 5 : 6)) - 1) / (kBM >> (v.inner <= 32 ? 5 : 6));
+    else tiles_m = v.outer * ((v.inner + kBM - 1) / kBM);
+    return tiles_m * jblocks;
+}
+
 cudaError_t launch_tc_single(const View3& v, cudaStream_t s, int* kid)
 {
     *kid = K_TC_BF16X3;

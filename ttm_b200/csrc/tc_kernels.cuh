@@ -13,6 +13,9 @@ bool tc_supported(const View3& v, int precision);
 // else K_TC_BF16X3 (the operand-split kernel and the single-SM kernel).
 cudaError_t launch_tc(const View3& v, int precision, cudaStream_t s, int* kid);
 
+// Output tiles of the single-SM bf16x3 kernel for this view (128 rows x up to 256 columns each).
+int64_t tc_single_tiles(const View3& v);
+
 // The single-SM bf16x3 kernel (and its operand split) whatever the shape.
 cudaError_t launch_tc_single(const View3& v, cudaStream_t s, int* kid);
 
