@@ -259,12 +259,13 @@ def run_extra_workloads(dev, stream):
     return out
 
 
-# DRAM bytes of one tc_bf16x3 launch, from one ncu capture of the same kernel on A (256,256,256,16)
-# (q = 2, m = 256): 1.074104 GB read + 1.018911 GB written. Traffic grows in proportion to the
-# slices processed, so a full S^4 launch moves that times S^4 / (256^3 * 16).
-CAPTURED_TRAFFIC = 1.074104e9 + 1.018911e9
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of tc_bf16x3 on A (256,256,256,16) "
-                  "q=2 m=256, scaled by the elements processed")
+# DRAM bytes of one launch of the bf16x3 kernel this workload runs (the pair kernel), from one ncu
+# capture of the same kernel on A (256,256,256,16) (q = 2, m = 256): 1.074166 GB read + 1.016612 GB
+# written. Traffic grows in proportion to the slices processed, so a full S^4 launch moves that
+# times S^4 / (256^3 * 16).
+CAPTURED_TRAFFIC = 1.074166e9 + 1.016612e9
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of tc_pair_kernel (tc_bf16x3_pair) on "
+                  "A (256,256,256,16) q=2 m=256, scaled by the elements processed")
 
 
 def traffic_per_launch(S):
