@@ -12,12 +12,16 @@
  *  2. high-level ttm(q, A, B, ep,sp,fp) -> tensor                     (reference ttm.h:100-125)
  *  3. operator   A(q) * B -> tensor                                    (reference ttm.h:133-138)
  *
+ * Interfaces 2 and 3 also take device_tensor (detail/device_tensor.h), whose elements stay in
+ * GPU memory: the product then runs with no host copies and returns a device_tensor.
+ *
  * The pointers of interface 1 may be host or device memory; the call blocks
  * until C is written. The policy tags are accepted for compatibility and do
  * not change the result (see detail/tags.h).
  */
 #pragma once
 
+#include "detail/device_tensor.h"
 #include "detail/tags.h"
 #include "detail/tensor.h"
 #include "detail/ttm.h"
@@ -62,11 +66,41 @@ inline auto ttm(std::size_t q, ttm::tensor<value_t> const& a, ttm::tensor<value_
     return c;
 }
 
+/** High-level interface on device-resident tensors: the same checks and texts as above; C is
+ *  made on the device (A's layout, nc[q-1] = nb[0]) and written by the product, with no host copy. */
+template <class value_t, class execution_policy, class slicing_policy, class fusion_policy>
+inline auto ttm(std::size_t q, ttm::device_tensor<value_t> const& a, ttm::device_tensor<value_t> const& b,
+                execution_policy ep, slicing_policy sp, fusion_policy fp)
+{
+    auto const p = a.order();
+    if (p == 0) throw std::runtime_error("Error in tlib::tensor_times_matrix: input tensor order should be greater zero.");
+    if (q == 0 || q > p) throw std::runtime_error("Error in tlib::tensor_times_matrix: contraction mode should be greater zero or less than or equal to p.");
+
+    auto nc = a.shape();
+    auto nb = b.shape();
+    nc[q - 1] = nb.at(0);
+    auto c = device_tensor<value_t>::uninitialized(nc, a.layout());
+
+    ttm(ep, sp, fp, static_cast<unsigned>(q), static_cast<unsigned>(p),
+        a.data(), a.shape().data(), a.strides().data(), a.layout().data(),
+        b.data(), b.shape().data(), b.layout().data(),
+        c.data(), c.shape().data(), c.strides().data());
+    return c;
+}
+
 } // namespace tlib::ttm
 
 /** Operator interface: C = A(q) * B, with the combined policies (reference ttm.h:133-138). */
 template <class value_t>
 inline auto operator*(tlib::ttm::tensor_view<value_t> const& a, tlib::ttm::tensor<value_t> const& b)
+{
+    return tlib::ttm::ttm(a.contraction_mode(), a.get_tensor(), b, tlib::ttm::parallel_policy::combined,
+                          tlib::ttm::slicing_policy::combined, tlib::ttm::fusion_policy::all);
+}
+
+/** Operator interface on device-resident tensors: C = A(q) * B stays on the device. */
+template <class value_t>
+inline auto operator*(tlib::ttm::device_tensor_view<value_t> const& a, tlib::ttm::device_tensor<value_t> const& b)
 {
     return tlib::ttm::ttm(a.contraction_mode(), a.get_tensor(), b, tlib::ttm::parallel_policy::combined,
                           tlib::ttm::slicing_policy::combined, tlib::ttm::fusion_policy::all);

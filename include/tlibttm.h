@@ -285,6 +285,22 @@ int tlibttm_synchronize(void* stream);
 int tlibttm_release_buffers(void);
 
 /*
+ * Device memory for callers built without the CUDA headers; the device-resident
+ * tlib::ttm::device_tensor (include/tlib/detail/device_tensor.h) is written on these.
+ *   tlibttm_device_alloc  bytes of memory on the current device (*ptr = NULL when bytes == 0);
+ *                         goes through the library's allocator, so FAIL_ALLOC applies
+ *                         (TLIBTTM_ERR_ALLOC)
+ *   tlibttm_device_free   frees what tlibttm_device_alloc returned (NULL is a no-op)
+ *   tlibttm_copy          synchronous copy of `bytes` between any mix of host and device memory
+ *   tlibttm_fill          sets `count` elements of type `dtype` (tlibttm_dtype) at device pointer
+ *                         `ptr` to `value`, enqueued on `stream`
+ */
+int tlibttm_device_alloc(void** ptr, size_t bytes);
+int tlibttm_device_free(void* ptr);
+int tlibttm_copy(void* dst, const void* src, size_t bytes);
+int tlibttm_fill(int dtype, void* ptr, size_t count, double value, void* stream);
+
+/*
  * Layout / stride helpers with the reference's semantics, for callers that
  * build metadata without the C++ header:
  *   tlibttm_k_order_layout  reference include/tlib/detail/layout.h:57-76

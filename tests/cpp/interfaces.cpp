@@ -10,6 +10,8 @@
 
 #include <cuda_runtime.h>
 
+#include "check.h"
+
 #include <cmath>
 #include <cstdio>
 #include <numeric>
@@ -17,61 +19,6 @@
 #include <vector>
 
 using namespace tlib::ttm;
-
-static int g_fail = 0;
-
-static void check(bool ok, const std::string& what)
-{
-    if (!ok) {
-        std::printf("FAIL %s\n", what.c_str());
-        ++g_fail;
-    }
-}
-
-// C = A x_q B from the definition, on strided host arrays (B column-major when b_cm).
-template <class T>
-static std::vector<T> naive(unsigned q, const std::vector<std::size_t>& na, const std::vector<std::size_t>& wa,
-                            const T* a, const T* b, bool b_cm, std::size_t m, const std::vector<std::size_t>& wc,
-                            std::size_t nc_elems)
-{
-    const unsigned p = (unsigned)na.size();
-    std::vector<T> c(nc_elems, T(0));
-    std::vector<std::size_t> idx(p, 0);
-    const std::size_t nq = na[q - 1];
-    std::size_t total = 1;
-    for (unsigned r = 0; r < p; ++r)
-        if (r != q - 1) total *= na[r];
-    for (std::size_t t = 0; t < total; ++t) {
-        std::size_t rem = t, oa = 0, oc = 0;
-        for (unsigned r = 0; r < p; ++r) {
-            if (r == q - 1) continue;
-            const std::size_t i = rem % na[r];
-            rem /= na[r];
-            oa += i * wa[r];
-            oc += i * wc[r];
-        }
-        for (std::size_t j = 0; j < m; ++j) {
-            double s = 0;
-            for (std::size_t l = 0; l < nq; ++l)
-                s += (double)a[oa + l * wa[q - 1]] * (double)b[b_cm ? j + l * m : j * nq + l];
-            c[oc + j * wc[q - 1]] = (T)s;
-        }
-    }
-    return c;
-}
-
-template <class T>
-static bool close(const std::vector<T>& x, const std::vector<T>& y)
-{
-    if (x.size() != y.size()) return false;
-    double num = 0, den = 0;
-    for (std::size_t i = 0; i < x.size(); ++i) {
-        num += ((double)x[i] - y[i]) * ((double)x[i] - y[i]);
-        den += (double)y[i] * y[i];
-    }
-    const double tol = sizeof(T) == 4 ? 1e-6 : 1e-13;
-    return std::sqrt(num) <= tol * std::sqrt(den) + 1e-30;
-}
 
 template <class T>
 static void high_level_and_operator(const char* tname)

@@ -49,19 +49,30 @@ def test_reference_measure_program(cuda):
     assert ours.count("Performance :") == 12
 
 
-def test_cpp_program_of_all_three_interfaces(cuda, tmp_path):
+def _cpp_program(name, tmp_path):
     gxx = shutil.which("g++")
     if not gxx:
         pytest.skip("g++ not available")
     cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-    exe = tmp_path / "interfaces"
+    exe = tmp_path / name
     lib = os.path.join(ROOT, "ttm_b200")
     subprocess.run([gxx, "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), "-I",
-                    os.path.join(cuda_home, "include"), os.path.join(ROOT, "tests", "cpp", "interfaces.cpp"),
+                    os.path.join(cuda_home, "include"), os.path.join(ROOT, "tests", "cpp", name + ".cpp"),
                     "-o", str(exe), "-L", lib, "-ltlibttm_cuda", "-L", os.path.join(cuda_home, "lib64"), "-lcudart",
                     f"-Wl,-rpath,{lib}:{os.path.join(cuda_home, 'lib64')}"], check=True)
-    out = _run(str(exe))
+    return _run(str(exe))
+
+
+def test_cpp_program_of_all_three_interfaces(cuda, tmp_path):
+    out = _cpp_program("interfaces", tmp_path)
     assert "interfaces ok" in out, out
+
+
+def test_cpp_device_resident_tensor(cuda, tmp_path):
+    """tlib::ttm::device_tensor: A(q) * B and ttm(q, A, B, ...) on device-resident tensors give the
+    host interfaces' exact bits, keep C on the device, and keep the host tensor's error texts."""
+    out = _cpp_program("device_tensor", tmp_path)
+    assert "device_tensor ok" in out, out
 
 
 def test_top_level_ttmpy_module_runs_the_reference_calls(cuda):

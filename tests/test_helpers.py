@@ -117,6 +117,24 @@ def test_cpp_headers_compile_and_predicates(tmp_path):
     assert r.returncode == 0, r.returncode
 
 
+@pytest.mark.parametrize("name", ["interfaces", "device_tensor"])
+def test_cpp_test_programs_build_and_link(tmp_path, name):
+    """The C++ programs that tests/test_gpu_dropin.py runs on the GPU compile warning-free and
+    resolve every symbol against libtlibttm_cuda.so (device_tensor needs no CUDA header)."""
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("g++ not available")
+    cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    lib = os.path.join(ROOT, "ttm_b200")
+    exe = tmp_path / name
+    subprocess.run([gxx, "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), "-I",
+                    os.path.join(cuda_home, "include"), os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-o",
+                    str(exe), "-L", lib, "-ltlibttm_cuda", "-L", os.path.join(cuda_home, "lib64"), "-lcudart",
+                    f"-Wl,-rpath,{lib}:{os.path.join(cuda_home, 'lib64')}"], check=True)
+    r = subprocess.run(["ldd", "-r", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and "undefined symbol" not in r.stdout + r.stderr, r.stdout + r.stderr
+
+
 @pytest.mark.parametrize("name", ["interface1", "interface2", "interface3", "measure"])
 def test_reference_examples_built_unchanged(name):
     """The reference's own example programs, compiled unchanged against include/ and linked with

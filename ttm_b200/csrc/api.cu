@@ -1221,6 +1221,50 @@ int tlibttm_release_buffers(void)
     return TLIBTTM_OK;
 }
 
+int tlibttm_device_alloc(void** ptr, size_t bytes)
+{
+    if (!ptr) return fail(TLIBTTM_ERR_ARG, "tlibttm_device_alloc: ptr is null.");
+    *ptr = nullptr;
+    if (bytes == 0) return TLIBTTM_OK;
+    cudaError_t e = dev_malloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return cuda_fail(e, "tlibttm_device_alloc");
+    }
+    return TLIBTTM_OK;
+}
+
+int tlibttm_device_free(void* ptr)
+{
+    if (!ptr) return TLIBTTM_OK;
+    cudaError_t e = cudaFree(ptr);
+    return e == cudaSuccess ? TLIBTTM_OK : cuda_fail(e, "tlibttm_device_free");
+}
+
+int tlibttm_copy(void* dst, const void* src, size_t bytes)
+{
+    if (bytes == 0) return TLIBTTM_OK;
+    if (!dst || !src) return fail(TLIBTTM_ERR_ARG, "tlibttm_copy: null pointer.");
+    cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyDefault);
+    return e == cudaSuccess ? TLIBTTM_OK : cuda_fail(e, "tlibttm_copy");
+}
+
+int tlibttm_fill(int dtype, void* ptr, size_t count, double value, void* stream)
+{
+    if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
+    if (count == 0) return TLIBTTM_OK;
+    if (!ptr) return fail(TLIBTTM_ERR_ARG, "tlibttm_fill: null pointer.");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    Where w;
+    int rc = classify(ptr, dev, w);
+    if (rc) return rc;
+    if (w != Where::Device) return fail(TLIBTTM_ERR_ARG, "tlibttm_fill: ptr must be device memory of the current device.");
+    e = launch_fill(ptr, (int64_t)count, dtype, value, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? TLIBTTM_OK : cuda_fail(e, "fill");
+}
+
 int tlibttm_k_order_layout(size_t* layout, size_t p, size_t k)
 {
     if (!layout || p == 0) return fail(TLIBTTM_ERR_ARG, "Error in tlib::ttm::detail::compute_k_order: range provided by begin and end not correct!");

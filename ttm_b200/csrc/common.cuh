@@ -112,6 +112,8 @@ cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_colvec_ls(const View3& v, int dtype, int ls, cudaStream_t s);
 cudaError_t launch_rowdot(const View3& v, int dtype, cudaStream_t s);
 cudaError_t launch_strided(const StridedProblem& sp, int dtype, cudaStream_t s);
+// Sets n elements at p (float when dtype == 0, else double) to v.
+cudaError_t launch_fill(void* p, int64_t n, int dtype, double v, cudaStream_t s);
 
 // Grouped launch: `count` problems, `total` work items pulled from the device counter `queue`
 // (which must be zero at launch) by a persistent grid of `grid` blocks.

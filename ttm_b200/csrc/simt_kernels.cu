@@ -1320,4 +1320,23 @@ cudaError_t launch_strided(const StridedProblem& sp, int dtype, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) fill_kernel(T* __restrict__ p, int64_t n, T v)
+{
+    const int64_t step = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += step) p[i] = v;
+}
+
+cudaError_t launch_fill(void* p, int64_t n, int dtype, double v, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    int sms = 148;
+    cudaError_t e = sms_of_device(sms);
+    if (e != cudaSuccess) return e;
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), int64_t(sms) * 8);
+    if (dtype == 0) fill_kernel<float><<<(unsigned)blocks, 256, 0, s>>>(static_cast<float*>(p), n, float(v));
+    else fill_kernel<double><<<(unsigned)blocks, 256, 0, s>>>(static_cast<double*>(p), n, v);
+    return cudaGetLastError();
+}
+
 }  // namespace tlibttm

@@ -6,10 +6,14 @@
 
 Both functions run on the GPU through the C ABI (include/tlibttm.h); there is
 no CPU fallback. Inputs may be numpy arrays (results come back as numpy
-arrays, the call blocks) or torch CUDA tensors (results are torch CUDA
-tensors produced on the current torch stream, no host round trip).
+arrays, the call blocks) or device arrays: torch CUDA tensors, or any object
+that exposes ``__cuda_array_interface__`` (versions 0-3: CuPy, Numba, ...) or
+the DLPack protocol (``__dlpack__``). Device arrays are used in place, with
+no copy and no host round trip; results are torch CUDA tensors produced on
+the current torch stream (they expose both protocols in turn, so CuPy and
+others take them without a copy), or the caller's own array given as ``out``.
 
-Same contract as the reference binding, plus three widenings:
+Same contract as the reference binding, plus four widenings:
 
 * float32 as well as float64 (the reference binds only double,
   wrapped_ttm.cpp:229-230). Other dtypes are converted to float64, as
@@ -20,6 +24,8 @@ Same contract as the reference binding, plus three widenings:
   A's layout, as in the reference (wrapped_ttm.cpp:57-66).
 * B's own memory order is honoured (row- or column-major); the reference
   assumes row-major (wrapped_ttm.cpp:46).
+* device arrays in place (above): the reference binds numpy only and copies
+  every result into a new numpy array (wrapped_ttm.cpp:57-66).
 
 Error behaviour follows the reference: its own checks raise ValueError with
 the same texts (wrapped_ttm.cpp:37-53, 90-127); checks of tlib::ttm raise
@@ -39,6 +45,57 @@ except Exception:  # noqa: BLE001
 
 def _is_torch(x) -> bool:
     return torch is not None and isinstance(x, torch.Tensor)
+
+
+def _cai_layout(iface):
+    """(pointer, shape, element strides, numpy dtype) of a ``__cuda_array_interface__`` dict.
+
+    Strides None means C order (the interface's convention); byte strides must be whole
+    elements. Masked arrays are rejected.
+    """
+    if iface.get("mask") is not None:
+        raise ValueError("ttmpy: masked device arrays are not supported.")
+    shape = tuple(int(x) for x in iface["shape"])
+    dt = np.dtype(iface["typestr"])
+    ptr = int(iface["data"][0]) if iface.get("data") is not None else 0
+    st = iface.get("strides")
+    if st is None:
+        strides, acc = [], 1
+        for n in reversed(shape):
+            strides.append(acc)
+            acc *= n
+        strides = tuple(reversed(strides))
+    else:
+        if any(int(b) % dt.itemsize for b in st):
+            raise ValueError("ttmpy: device array strides must be whole elements.")
+        strides = tuple(int(b) // dt.itemsize for b in st)
+    return ptr, shape, strides, dt
+
+
+def _device_view(x):
+    """A torch tensor over the memory of ``x`` (no copy) when ``x`` is a device array given
+    through ``__cuda_array_interface__`` or DLPack; None for numpy arrays, torch tensors and
+    anything else.
+
+    A ``stream`` entry of the CUDA array interface (version 3) is honoured: the current torch
+    stream waits for the producer's stream before any library work reads the memory. DLPack
+    producers order their own work, given the consumer's stream by ``torch.from_dlpack``.
+    """
+    if torch is None or _is_torch(x) or isinstance(x, np.ndarray):
+        return None
+    iface = getattr(x, "__cuda_array_interface__", None)
+    if iface is not None:
+        _cai_layout(iface)
+        t = torch.as_tensor(x, device="cuda")
+        stream = iface.get("stream")
+        if stream is not None and int(stream) != 0:
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.ExternalStream(int(stream), device=t.device))
+            torch.cuda.current_stream(t.device).wait_event(ev)
+        return t
+    if hasattr(x, "__dlpack__"):
+        return torch.from_dlpack(x)
+    return None
 
 
 def _layout_from_strides(shape, strides):
@@ -72,9 +129,17 @@ def _check_q_p(q, p, fn):
         raise ValueError("Error calling ttmpy::ttms: input tensor order should be greater than zero.")
 
 
-def _ttm_numpy(q, A, B, precision):
+def _out_error(nc, wc, dt):
+    return ValueError(f"ttmpy: out must be an array of shape {tuple(nc)} and dtype {dt} laid out like A "
+                      f"(strides {tuple(wc)} in elements).")
+
+
+def _ttm_numpy(q, A, B, precision, out=None):
     if precision == "tuned":
         precision = "plain"
+    dB = B if _is_torch(B) else _device_view(B)
+    if dB is not None:
+        B = dB.detach().cpu().numpy()
     A = np.asarray(A)
     p = A.ndim
     _check_q_p(q, p, "ttm")
@@ -103,14 +168,21 @@ def _ttm_numpy(q, A, B, precision):
     nc = list(na)
     nc[q - 1] = nb[0]
     wc = _dense_strides(nc, pia)
-    C = np.lib.stride_tricks.as_strided(np.empty(int(np.prod(nc)), dtype=A.dtype), shape=nc,
-                                        strides=[w * A.itemsize for w in wc])
+    if out is None:
+        C = np.lib.stride_tricks.as_strided(np.empty(int(np.prod(nc)), dtype=A.dtype), shape=nc,
+                                            strides=[w * A.itemsize for w in wc])
+    else:
+        C = out
+        if (not isinstance(C, np.ndarray) or C.dtype != A.dtype or list(C.shape) != nc
+                or [st // C.itemsize for st in C.strides] != wc or not C.flags.writeable):
+            raise _out_error(nc, wc, A.dtype)
     _lib.ttm_raw(_dtype_id(A.dtype.type), _prec(precision), q, p, A.ctypes.data, na, wa, pia,
                  B.ctypes.data, nb, pib, C.ctypes.data, nc, wc, 0)
     return C
 
 
-def _ttm_torch(q, A, B, precision):
+def _ttm_torch(q, A, B, precision, out=None):
+    B_in = B
     p = A.dim()
     _check_q_p(q, p, "ttm")
     if q == 0 or q > p:
@@ -118,7 +190,9 @@ def _ttm_torch(q, A, B, precision):
     if A.dtype not in (torch.float32, torch.float64):
         A = A.to(torch.float64)
     if not _is_torch(B):
-        B = torch.as_tensor(np.asarray(B), device=A.device)
+        B = _device_view(B)
+        if B is None:
+            B = torch.as_tensor(np.asarray(B_in), device=A.device)
     if B.dim() != 2:
         raise ValueError("Error calling ttmpy::ttm: second input should be a mtrix with order equal to 2.")
     B = B.to(device=A.device, dtype=A.dtype)
@@ -138,7 +212,13 @@ def _ttm_torch(q, A, B, precision):
     nc = list(na)
     nc[q - 1] = nb[0]
     wc = _dense_strides(nc, pia)
-    C = torch.empty_strided(nc, wc, dtype=A.dtype, device=A.device)
+    if out is None:
+        C = torch.empty_strided(nc, wc, dtype=A.dtype, device=A.device)
+    else:
+        C = out if _is_torch(out) else _device_view(out)
+        if (C is None or C.dtype != A.dtype or C.device != A.device or list(C.shape) != nc
+                or list(C.stride()) != wc):
+            raise _out_error(nc, wc, str(A.dtype).replace("torch.", ""))
     stream = torch.cuda.current_stream(A.device).cuda_stream if A.is_cuda else 0
     if precision == "tuned" and A.is_cuda and _dense_strides(na, pia) == wa:
         # the learned schedule selector picks among the exact kernels (float32 may also take bf16x3)
@@ -163,7 +243,7 @@ def _ttm_torch(q, A, B, precision):
     return C
 
 
-def ttm(q, A, B, precision="default"):
+def ttm(q, A, B, precision="default", out=None):
     """Mode-q tensor-times-matrix product C = A x_q B (reference wrapped_ttm.cpp:23-76).
 
     C(i1..j..ip) = sum_{iq} A(i1..iq..ip) * B(j, iq); q is one-based.
@@ -171,11 +251,21 @@ def ttm(q, A, B, precision="default"):
     "auto", or "tuned"); "default" is the library-wide setting (plain unless
     changed). "tuned" lets the learned schedule selector pick the kernel for
     device tensors (FP32-accurate for float32, exact for float64).
+
+    ``out`` (optional) receives C in place and is returned: for device inputs a torch CUDA
+    tensor or any device array (CUDA array interface, DLPack) on A's device, for numpy inputs a
+    writeable numpy array; either way with C's shape, A's dtype and A's layout (the strides of
+    a dense array whose modes are ordered as A's). Anything else raises ValueError.
     """
     q = int(q)
+    dA = _device_view(A)
+    if dA is not None:
+        A = dA
     if _is_torch(A):
-        return _ttm_torch(q, A, B, precision)
-    return _ttm_numpy(q, A, B, precision)
+        C = _ttm_torch(q, A, B, precision, out)
+    else:
+        C = _ttm_numpy(q, A, B, precision, out)
+    return C if out is None else out
 
 
 def _ttms_check(q, A, Bs, order):
@@ -229,8 +319,15 @@ def ttms(q, A, Bs, order="forward", precision="default"):
     The whole chain runs as one plan (include/tlibttm.h, tlibttm_plan_chain):
     numpy inputs are moved to the GPU once, intermediates stay in device
     buffers the plan owns, and only the final tensor returns to the host.
+    Device arrays (torch, CUDA array interface, DLPack) are read in place and
+    the result is a torch CUDA tensor.
     """
     q = int(q)
+    dA = _device_view(A)
+    if dA is not None:
+        A = dA
+    views = [_device_view(b) for b in Bs]
+    Bs = [b if v is None else v for b, v in zip(Bs, views)]
     p = _ttms_check(q, A, Bs, order)
     seq = _ttms_sequence(q, p, Bs, order)
     if torch is None or not torch.cuda.is_available():
