@@ -59,13 +59,10 @@ def test_batched_plan_matches_references(cuda, dt, precision):
         got = pr["C"].double().cpu().numpy()
         worst = max(worst, np.linalg.norm(got - want) / np.linalg.norm(want))
     assert worst <= tol, worst
-    assert plan.launches >= 1
-    if precision == "plain":
-        # small-m problems of at least 2^18 elements run on their own (forked over the plan's
-        # worker streams); every other problem shares the one grouped launch
-        singles = sum(1 for pr in probs if pr["m"] <= 16 and int(np.prod(pr["na"])) >= 1 << 18)
-        grouped = len(probs) - singles
-        assert singles > 1 and plan.launches == (1 if grouped else 0) + singles
+    # grouped launches (tensor-core, TMA-fed small-m, SIMT) plus the few small-m problems the
+    # TMA-fed kernel does not take (unaligned rows) above the single-launch size
+    small_misaligned = sum(1 for pr in probs if pr["m"] <= 16 and int(np.prod(pr["na"])) >= 1 << 18)
+    assert 1 <= plan.launches <= 16 + small_misaligned
     plan.close()
 
 
@@ -116,3 +113,112 @@ def test_plan_errors_name_the_problem(cuda):
     probs[1] = dict(probs[1], m=0)        # C would have a zero extent
     with pytest.raises(_lib.TtmError, match="problem 1: Error in tlib::tensor_times_matrix: shape vector of C is not valid"):
         BatchPlan(probs, precision="plain")
+
+
+# (na, pia, q, m): every geometry and mode of the bf16x3 kernel in one grouped launch
+GROUPED_TC_CASES = [
+    ([256, 40, 6], [1, 2, 3], 2, 64),      # rows of i, TMA tiles
+    ([200, 33, 5], [1, 2, 3], 2, 130),     # rows of i, a partial last tile, N = 144
+    ([20, 48, 30], [1, 2, 3], 2, 17),      # inner <= 32: four slices folded into a 128-row tile
+    ([50, 20, 30], [1, 2, 3], 2, 256),     # inner <= 64: two slices per tile
+    ([130, 24, 7], [1, 2, 3], 2, 40),      # inner % 4 != 0: the converters load A, C stored directly
+    ([36, 300, 4], [2, 1, 3], 2, 300),     # contiguous fibres, two j blocks (m > 256)
+    ([30, 64, 50], [2, 1, 3], 2, 96),      # contiguous fibres (q = pi_1)
+    ([11, 37, 90], [2, 1, 3], 2, 18),      # fibres with n_q % 4 != 0 (converters load), m % 4 != 0
+    ([64, 64, 64], [3, 1, 2], 1, 200),     # another layout
+]
+
+
+def test_grouped_bf16x3_launch_matches_single_launches(cuda):
+    """Under auto every float problem with m > 16 that the tensor-core path takes joins one grouped
+    bf16x3 launch: one operand split for all B plus one persistent launch per geometry (3 here).
+    Each result equals the single-SM bf16x3 kernel's (schedule 5) bit for bit, run before and
+    after new data are written into the same buffers (graph replay)."""
+    import ctypes as C
+    import torch
+    from ttm_b200.plans import BatchPlan
+    from ttm_b200.selector import lib as sched_lib
+    g = torch.Generator(device=cuda).manual_seed(7)
+    probs = []
+    for na, pia, q, m in GROUPED_TC_CASES:
+        n = int(np.prod(na))
+        probs.append(dict(q=q, na=na, pia=pia, m=m, A=torch.randn(n, device=cuda, generator=g),
+                          B=torch.randn(m, na[q - 1], device=cuda, generator=g),
+                          C=torch.full((n // na[q - 1] * m,), float("nan"), device=cuda)))
+    plan = BatchPlan(probs, precision="auto")
+    assert plan.launches == 3
+
+    def single(pr):
+        na, pia, q, m = pr["na"], pr["pia"], pr["q"], pr["m"]
+        nc = list(na)
+        nc[q - 1] = m
+        out = torch.full_like(pr["C"], float("nan"))
+        _lib.check(sched_lib().tlibttm_ttm_sched(_lib.F32, 5, q, len(na), C.c_void_p(pr["A"].data_ptr()), _lib.sz(na),
+                                                 _lib.sz(ka.dense_strides(na, pia)), _lib.sz(pia),
+                                                 C.c_void_p(pr["B"].data_ptr()), _lib.sz([m, na[q - 1]]),
+                                                 _lib.sz([2, 1]), C.c_void_p(out.data_ptr()), _lib.sz(nc),
+                                                 _lib.sz(ka.dense_strides(nc, pia)),
+                                                 C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return out
+
+    for rnd in range(2):
+        plan.run_graph()
+        torch.cuda.synchronize()
+        assert _lib.lib().tlibttm_synchronize(None) == 0
+        for i, pr in enumerate(probs):
+            want = single(pr)
+            torch.cuda.synchronize()
+            assert torch.equal(pr["C"], want), (rnd, GROUPED_TC_CASES[i])
+            ref = _ref(pr["A"].double().cpu().numpy(), pr["na"], pr["pia"], pr["q"], pr["B"].double().cpu().numpy())
+            err = np.linalg.norm(pr["C"].double().cpu().numpy() - ref) / np.linalg.norm(ref)
+            assert err <= 1e-5, (GROUPED_TC_CASES[i], err)
+        for pr in probs:                   # new A and B in the same buffers
+            pr["A"].mul_(-0.5)
+            pr["B"].add_(1.0)
+    plan.close()
+
+
+# (na, pia, q, m): row mode (contiguous fibres) and column mode with each box shape, every MB build
+GROUPED_STREAM_CASES = [
+    ([64, 300, 50], [2, 1, 3], 2, 1),      # contiguous fibres (q = pi_1), n_q % 4 == 0
+    ([40, 64, 90], [2, 1, 3], 2, 7),       # contiguous fibres, MB 8
+    ([36, 128, 60], [2, 1, 3], 2, 16),     # contiguous fibres, MB 16
+    ([1024, 30, 20], [1, 2, 3], 2, 2),     # strided fibres, wide rows of i
+    ([12, 50, 500], [1, 2, 3], 2, 3),      # inner 12: many slices per box
+    ([256, 8, 70], [1, 2, 3], 2, 5),       # short n_q
+    ([384, 40, 33], [1, 2, 3], 2, 11),     # MB 16, one CTA per SM
+    ([64, 64, 64], [3, 1, 2], 2, 4),       # another layout
+    ([20, 90, 64], [1, 3, 2], 3, 9),
+]
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64"])
+def test_grouped_small_m_launch(cuda, dt):
+    """Every dense problem with m <= 16 that the TMA-fed kernel takes with B staged whole joins one
+    grouped launch per (row/column mode, MB build, CTAs per SM) class: here 9 problems in at most 9
+    launches, replayed as a graph with new data; exact FMA arithmetic, so each result is within the
+    exact-path bound of the FP64 reference (2e-6 float, 1e-13 double)."""
+    import torch
+    from ttm_b200.plans import BatchPlan
+    dtype = torch.float32 if dt == "f32" else torch.float64
+    g = torch.Generator(device=cuda).manual_seed(9)
+    probs = []
+    for na, pia, q, m in GROUPED_STREAM_CASES:
+        n = int(np.prod(na))
+        probs.append(dict(q=q, na=na, pia=pia, m=m, A=torch.randn(n, device=cuda, dtype=dtype, generator=g),
+                          B=torch.randn(m, na[q - 1], device=cuda, dtype=dtype, generator=g),
+                          C=torch.full((n // na[q - 1] * m,), float("nan"), device=cuda, dtype=dtype)))
+    plan = BatchPlan(probs, precision="plain")
+    assert 1 <= plan.launches <= len(GROUPED_STREAM_CASES)
+    tol = 2e-6 if dt == "f32" else 1e-13
+    for rnd in range(2):
+        plan.run_graph()
+        torch.cuda.synchronize()
+        for i, pr in enumerate(probs):
+            ref = _ref(pr["A"].double().cpu().numpy(), pr["na"], pr["pia"], pr["q"], pr["B"].double().cpu().numpy())
+            err = np.linalg.norm(pr["C"].double().cpu().numpy() - ref) / np.linalg.norm(ref)
+            assert err <= tol, (rnd, GROUPED_STREAM_CASES[i], err)
+        for pr in probs:
+            pr["A"].mul_(1.5)
+            pr["B"].sub_(0.25)
+    plan.close()

@@ -643,6 +643,8 @@ struct tlibttm_plan_s {
     int64_t total = 0;
     int grid = 0;
     std::vector<tlibttm::Single> singles;   // individual launches (batched extras, or chain steps)
+    tlibttm::TcGroup* tcg = nullptr;         // batched: the grouped bf16x3 launch
+    tlibttm::StreamGroup* sg = nullptr;      // batched: the grouped small-m launch
     // chain
     void* bufs[2] = {nullptr, nullptr};
     // graph
@@ -664,7 +666,10 @@ int plan_run_impl(tlibttm_plan* P, cudaStream_t s)
     cudaError_t e;
     // Batched plans with several singles fork them over worker streams (largest first, round
     // robin) and join them back into s; chain plans run their steps in order on s.
-    const bool fan = P->type == 0 && P->singles.size() > 1;
+    // The grouped bf16x3 launch takes worker stream 0 and the singles the others, so that they
+    // run side by side.
+    const bool fan = P->type == 0 && (P->singles.size() > 1 || (P->tcg && !P->singles.empty()));
+    const int w0 = (fan && P->tcg) ? 1 : 0;   // first worker stream of the singles
     if (fan) {
         if (!P->fork) {
             if ((e = cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming)) != cudaSuccess)
@@ -678,6 +683,14 @@ int plan_run_impl(tlibttm_plan* P, cudaStream_t s)
         for (int w = 0; w < kPlanStreams; ++w)
             if ((e = cudaStreamWaitEvent(P->workers[w], P->fork, 0)) != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
     }
+    if (P->tcg) {
+        if ((rc = note_launch(tc_group_run(P->tcg, fan ? P->workers[0] : s), K_TC_BF16X3))) return rc;
+        g_launches += (unsigned long long)(tc_group_launches(P->tcg) - 1);
+    }
+    if (P->sg && stream_group_launches(P->sg) > 0) {
+        if ((rc = note_launch(stream_group_run(P->sg, s), K_STREAM_COLS))) return rc;
+        g_launches += (unsigned long long)(stream_group_launches(P->sg) - 1);
+    }
     if (P->type == 0 && P->total > 0) {
         e = cudaMemsetAsync(P->d_queue, 0, sizeof(unsigned long long), s);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -686,7 +699,9 @@ int plan_run_impl(tlibttm_plan* P, cudaStream_t s)
             return rc;
     }
     for (size_t i = 0; i < P->singles.size(); ++i)
-        if ((rc = run_single(P->singles[i], P->precision, fan ? P->workers[i % kPlanStreams] : s))) return rc;
+        if ((rc = run_single(P->singles[i], P->precision,
+                             fan ? P->workers[w0 + (int)(i % (size_t)(kPlanStreams - w0))] : s)))
+            return rc;
     if (fan) {
         for (int w = 0; w < kPlanStreams; ++w) {
             if ((e = cudaEventRecord(P->joins[w], P->workers[w])) != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
@@ -703,6 +718,8 @@ void plan_free(tlibttm_plan* P)
     if (P->graph) cudaGraphDestroy(P->graph);
     if (P->d_desc) cudaFree(P->d_desc);
     if (P->d_queue) cudaFree(P->d_queue);
+    tc_group_destroy(P->tcg);
+    stream_group_destroy(P->sg);
     for (void* b : P->bufs)
         if (b) cudaFree(b);
     if (P->own) cudaStreamDestroy(P->own);
@@ -900,6 +917,8 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
     const int64_t tile = dtype == TLIBTTM_F32 ? kGemmTileF32 : kGemmTileF64;
     struct Item { GroupDesc d; double cost; };
     std::vector<Item> items;
+    std::vector<View3> tcviews;   // problems of the grouped bf16x3 launch
+    std::vector<View3> sgviews;   // problems of the grouped small-m (TMA-fed) launch
     for (size_t i = 0; i < count; ++i) {
         const tlibttm_problem& pr = problems[i];
         Args x{dtype, pr.q, pr.p, pr.a, pr.na, pr.wa, pr.pia, pr.b, pr.nb, pr.pib, pr.c, pr.nc, pr.wc};
@@ -929,14 +948,19 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                         }
                         single = true;
                     }
-                    if (pl.dense && v.m > kSmallM && dtype == TLIBTTM_F32) {
-                        // bf16x3 asked for explicitly: every supported problem takes it; under auto,
-                        // supported problems above the single-launch size
-                        if (prec == TLIBTTM_PREC_BF16X3) single = tc_supported(v, TLIBTTM_PREC_BF16X3);
-                        if (prec == TLIBTTM_PREC_AUTO)
-                            single = tc_supported(v, TLIBTTM_PREC_BF16X3) && elems >= kPlanSingleMinElems;
+                    if (pl.dense && v.m > kSmallM && dtype == TLIBTTM_F32 &&
+                        (prec == TLIBTTM_PREC_BF16X3 || prec == TLIBTTM_PREC_AUTO) && tc_supported(v, TLIBTTM_PREC_BF16X3)) {
+                        // bf16x3 (asked for, or chosen by auto as a single call would): every such
+                        // problem joins the grouped tensor-core launch
+                        tcviews.push_back(v);
+                        continue;
                     }
-                    // small m: the small-m kernels (column, row, TMA-fed) above the single-launch size
+                    // small m: the grouped TMA-fed launch where it takes the problem, else the small-m
+                    // kernels (column, row) above the single-launch size
+                    if (pl.dense && v.m <= kSmallM && stream_group_eligible(v, dtype)) {
+                        sgviews.push_back(v);
+                        continue;
+                    }
                     if (pl.dense && v.m <= kSmallM && elems >= kPlanSingleMinElems) single = true;
                     if (!pl.dense || single) {
                         P->singles.push_back(Single{dtype, x.a, x.b, x.c, pl});
@@ -1013,6 +1037,12 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
         const int64_t grid = (int64_t)sms * grouped_blocks_per_sm(dtype);
         P->grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, P->total));
     }
+    if (!tcviews.empty() && (e = tc_group_create(tcviews.data(), (int)tcviews.size(), &P->tcg)) != cudaSuccess)
+        return e == cudaErrorMemoryAllocation ? fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_batched: device allocation failed.")
+                                              : cuda_fail(e, "grouped bf16x3 set-up");
+    if (!sgviews.empty() && (e = stream_group_create(sgviews.data(), (int)sgviews.size(), dtype, &P->sg)) != cudaSuccess)
+        return e == cudaErrorMemoryAllocation ? fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_batched: device allocation failed.")
+                                              : cuda_fail(e, "grouped small-m set-up");
     if (!P->singles.empty() && (e = tc_prepare_device()) != cudaSuccess) return cuda_fail(e, "tensor-core state");
     *plan = P.release();
     return TLIBTTM_OK;
@@ -1142,6 +1172,7 @@ int tlibttm_plan_launches(const tlibttm_plan* plan)
 {
     if (!plan) return 0;
     int n = (plan->type == 0 && plan->total > 0) ? 1 : 0;
+    n += tc_group_launches(plan->tcg) + stream_group_launches(plan->sg);
     for (const Single& sg : plan->singles) n += launches_of(sg, plan->dtype, plan->precision);
     return n;
 }

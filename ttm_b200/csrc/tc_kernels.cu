@@ -26,12 +26,15 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <type_traits>
 #include <unordered_map>
+#include <vector>
 
 #include "tc_kernels.cuh"
 #include "tc_ptx.cuh"
@@ -89,24 +92,41 @@ __device__ __forceinline__ uint32_t mnmaj_sw128_off(uint32_t l, uint32_t ichunk)
     return atom * 1024u + row * 128u + ((c ^ row) << 4);
 }
 
-struct TcParams {
+// One problem of a bf16x3 launch: its tensor maps, pointers and tiling. A single launch passes it
+// as a kernel parameter; a grouped launch reads an array of them from device memory (64-byte
+// aligned, as TMA requires of a tensor map), ordered by `first`.
+struct alignas(64) TcProb {
+    CUtensorMap amap;        // A tiles (unused when ldg_a)
+    CUtensorMap cmap;        // 32 x 32 blocks of C for the TMA-store epilogue (unused when !tma_c)
     float* c;
     const float* a;          // A itself, for the converters' own loads (ldg_a)
-    int ldg_a;               // A rows not 16-byte aligned for TMA: the converters load A
-    int fold_kb;             // GEOM_MN with inner <= 64: slices per 128-row tile (1: unfolded)
-    int fold_ib_shift;       // log2 of the rows each slice takes in a folded tile (32 or 64)
+    const float* b;          // B itself, read by the operand split
     const uint8_t* bimg;     // pre-split B: [jb][kc][hi|lo][NT rows x 32 B]
-    int* status;             // device status word (0 = ok)
     int64_t outer, nq, inner, m;
     int64_t tiles_m;         // M tiles per j block
-    int64_t tiles;           // total tiles
+    int64_t tiles;           // tiles of this problem
+    int64_t first;           // grouped launch: index of its first tile among all problems' tiles
     int nt;                  // MMA N (multiple of 16, <= 256)
     int jblocks;
     int kchunks;             // 16-l sub-blocks of n_q
     int kstages;             // pipeline stages per tile: ceil(kchunks / kSub)
+    int ldg_a;               // A rows not 16-byte aligned for TMA: the converters load A
+    int tma_c;               // epilogue stores C through the C tensor map
+    int fold_kb;             // GEOM_MN with inner <= 64: slices per 128-row tile (1: unfolded)
+    int fold_ib_shift;       // log2 of the rows each slice takes in a folded tile (32 or 64)
+    int b_cm;
+};
+
+// Launch-wide parameters.
+struct TcParams {
+    int* status;             // device status word (0 = ok)
+    const TcProb* group;     // grouped launch: `count` problems in device memory (else unused)
+    int count;
+    int64_t total;           // tiles over all problems of the launch
     int fstages;             // A ring depth (FP32 tile, converted in place)
     int ostages;             // B ring depth
-    int tma_c;               // epilogue stores C through the C tensor map
+    uint32_t bslot;          // bytes of one B ring slot (the largest B stage of the launch)
+    int acc_stride;          // tensor-memory columns between the two accumulators
     int skip_b;              // test of the bounded waits: the B producer skips its first stage
     unsigned long long wait_ns;   // bound of the pipeline's mbarrier waits
 };
@@ -140,13 +160,21 @@ __host__ inline bool choose_stages(int nt, int& as, int& bs, size_t& smem)
 {
     const SmemLayout L = smem_layout(nt);
     const size_t avail = kSmemBudget - 1024 - kCtrlBytes - kEpiBytes;
-    // at least kConvGroups A stages: each converter group waits on its own stage's barrier by
-    // phase parity, which stays unambiguous only while the groups cover at most one ring pass
+    // A stages: a multiple of kConvGroups. Group g converts the stages n = g (mod kConvGroups) in
+    // order, waiting on each stage's barrier by phase parity; with the ring a multiple of the
+    // groups every slot belongs to one group, which sees each phase of it in turn. Otherwise a
+    // group could wait on a slot whose previous load (another group's) has not landed yet -- loads
+    // may land out of order -- and the parity of that pending phase would read as the completed
+    // one before it.
+    // B stages (from L2) give way first, down to two, so that A keeps two stages per group
+    // (measured at N = 256: 8 A + 2 B stages beat 4 + 3 by 10 %)
     bs = kMaxB;
+    while (bs > 2 && (size_t)bs * L.bstage_bytes + 2 * kConvGroups * L.a_bytes > avail) --bs;
     while (bs > 2 && (size_t)bs * L.bstage_bytes + kConvGroups * L.a_bytes > avail) --bs;
     if ((size_t)bs * L.bstage_bytes + kConvGroups * L.a_bytes > avail) return false;
     as = (int)((avail - (size_t)bs * L.bstage_bytes) / L.a_bytes);
     if (as > kMaxA) as = kMaxA;
+    as -= as % kConvGroups;
     smem = 1024 + (size_t)as * L.a_bytes + (size_t)bs * L.bstage_bytes + kEpiBytes + kCtrlBytes;
     return true;
 }
@@ -159,17 +187,44 @@ __device__ __forceinline__ void conv_barrier(int g)
     asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "n"(kGroupWarps * 32) : "memory");
 }
 
-template <int GEOM>
+// The problem owning tile t of the launch, and the tile's index within that problem. A role
+// visits its tiles in increasing order, so the search goes on from the problem of its previous
+// tile (`cur`, 0 at the start).
+template <bool GROUP>
+__device__ __forceinline__ const TcProb& tile_problem(const TcProb& one, const TcParams& P, int64_t t, int& cur,
+                                                      int64_t& lt)
+{
+    if constexpr (!GROUP) {
+        lt = t;
+        return one;
+    } else {
+        while (cur + 1 < P.count && P.group[cur + 1].first <= t) ++cur;
+        lt = t - P.group[cur].first;
+        return P.group[cur];
+    }
+}
+
+// A tensor map in device memory is read through the tensor-map proxy: order that read after the
+// generic-proxy writes that made the map (the plan's upload) before the first copy using it.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+// GROUP = false: one problem, `one`. GROUP = true: the P.count problems of P.group, whose tiles
+// are numbered one after the other; every role walks the same tile sequence, so the pipeline
+// runs across problem boundaries without draining.
+template <int GEOM, bool GROUP>
 __global__ void __launch_bounds__(kThreads, 1)
-    tc_bf16x3_kernel(const __grid_constant__ CUtensorMap amap, const __grid_constant__ CUtensorMap cmap, TcParams P)
+    tc_bf16x3_kernel(const __grid_constant__ TcProb one, TcParams P)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const SmemLayout L = smem_layout(P.nt);
+    const SmemLayout LA = smem_layout(kMaxNT);   // its A sizes do not depend on N
     const int AS = P.fstages, BS = P.ostages;
     uint8_t* aring = smem;
-    uint8_t* bring = smem + (size_t)AS * L.a_bytes;
-    uint8_t* epi = bring + (size_t)BS * L.bstage_bytes;
+    uint8_t* bring = smem + (size_t)AS * LA.a_bytes;
+    uint8_t* epi = bring + (size_t)BS * P.bslot;
     uint8_t* ctrl = epi + kEpiBytes;
     uint64_t* a_full = reinterpret_cast<uint64_t*>(ctrl);   // [AS]  TMA of the FP32 tile landed
     uint64_t* a_conv = a_full + kMaxA;                        // [AS]  bf16 hi/lo written in place
@@ -183,8 +238,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    auto a_at = [&](int s) { return aring + (size_t)s * L.a_bytes; };
-    auto bhi_at = [&](int s) { return bring + (size_t)s * L.bstage_bytes; };
+    auto a_at = [&](int s) { return aring + (size_t)s * LA.a_bytes; };
+    auto bhi_at = [&](int s) { return bring + (size_t)s * P.bslot; };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < AS; ++s) {
@@ -214,9 +269,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int64_t tiles = P.tiles;
-    const int kstages = P.kstages;
-    const int64_t mper = (P.inner + kBM - 1) / kBM;
+    const int64_t tiles = P.total;
 
     if (warp == 0) {
         // ------------------------------------------------------------- A producer (TMA)
@@ -226,31 +279,41 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool ok = true;
             int issued[kMaxA];
             for (int i = 0; i < kMaxA; ++i) issued[i] = -1;
+            const TcProb* last = nullptr;
+            int cur = 0;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                const int64_t mt = t % P.tiles_m;
-                for (int st = 0; st < kstages; ++st) {
+                int64_t lt;
+                const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
+                if (GROUP && &pr != last && !pr.ldg_a) tensormap_acquire(&pr.amap);
+                last = &pr;
+                const int64_t mt = lt % pr.tiles_m, mper = (pr.inner + kBM - 1) / kBM;
+                for (int st = 0; st < pr.kstages; ++st) {
                     if (!mbar_wait(&a_empty[s], ph ^ 1, abort_flag, P.wait_ns)) { ok = false; break; }
-                    if (P.ldg_a) {
-                        // no copy: the stage is free for the converters, which load A themselves
+                    if (pr.ldg_a) {
+                        // no copy: the stage is free for the converters, which load A themselves.
+                        // No copy is in flight into it either (its last one landed before the
+                        // stage was freed), so the final drain must not wait on it: a phase
+                        // recorded by an earlier copy would by then be ambiguous by parity.
+                        issued[s] = -1;
                         mbar_arrive(&a_full[s]);
                         if (++s == AS) { s = 0; ph ^= 1; }
                         continue;
                     }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&a_full[s], L.a_bytes);
+                    mbar_expect_tx(&a_full[s], LA.a_bytes);
                     // kSub boxes; a box past n_q (odd chunk count) is zero-filled by the copy
 #pragma unroll
                     for (int sub = 0; sub < kSub; ++sub) {
-                        uint8_t* dst = a_at(s) + sub * L.asub_bytes;
+                        uint8_t* dst = a_at(s) + sub * LA.asub_bytes;
                         const int l0 = (st * kSub + sub) * kBK;
-                        if (GEOM == GEOM_MN && P.fold_kb > 1) {
+                        if (GEOM == GEOM_MN && pr.fold_kb > 1) {
                             // folded tile: slices mt*KB .. +KB-1, the map ordered (i, k, l)
-                            tma_load_3d(dst, &amap, &a_full[s], 0, (int)(mt * P.fold_kb), l0);
+                            tma_load_3d(dst, &pr.amap, &a_full[s], 0, (int)(mt * pr.fold_kb), l0);
                         } else if (GEOM == GEOM_MN) {
                             const int64_t k = mt / mper, ib = mt - k * mper;
-                            tma_load_3d(dst, &amap, &a_full[s], (int)(ib * kBM), l0, (int)k);
+                            tma_load_3d(dst, &pr.amap, &a_full[s], (int)(ib * kBM), l0, (int)k);
                         } else {
-                            tma_load_2d(dst, &amap, &a_full[s], l0, (int)(mt * kBM));
+                            tma_load_2d(dst, &pr.amap, &a_full[s], l0, (int)(mt * kBM));
                         }
                     }
                     if (++s == AS) { s = 0; ph ^= 1; }
@@ -271,9 +334,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool ok = true;
             int issued[kMaxB];
             for (int i = 0; i < kMaxB; ++i) issued[i] = -1;
+            int cur = 0;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                const int64_t jb = t / P.tiles_m;
-                for (int st = 0; st < kstages; ++st) {
+                int64_t lt;
+                const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
+                const SmemLayout Lp = smem_layout(pr.nt);
+                const int64_t jb = lt / pr.tiles_m;
+                for (int st = 0; st < pr.kstages; ++st) {
                     if (!mbar_wait(&b_empty[s], ph ^ 1, abort_flag, P.wait_ns)) { ok = false; break; }
                     if (P.skip_b && t == blockIdx.x && st == 0) {
                         // test of the bounded waits: this stage is never filled (no copy, no arrive)
@@ -281,10 +348,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                         continue;
                     }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&b_full[s], L.bstage_bytes);
+                    mbar_expect_tx(&b_full[s], Lp.bstage_bytes);
                     // the image holds kstages * kSub sub-blocks per j block: one copy per stage
-                    const uint8_t* img = P.bimg + ((size_t)(jb * kstages + st) * L.bstage_bytes);
-                    bulk_load(bhi_at(s), img, L.bstage_bytes, &b_full[s]);
+                    const uint8_t* img = pr.bimg + ((size_t)(jb * pr.kstages + st) * Lp.bstage_bytes);
+                    bulk_load(bhi_at(s), img, Lp.bstage_bytes, &b_full[s]);
                     if (++s == BS) { s = 0; ph ^= 1; }
                 }
             }
@@ -299,7 +366,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         // The whole warp runs the loop (warp-uniform descriptors); one elected lane issues each
         // MMA and commit; wait results are made warp-uniform before they steer the loop.
         {
-            const uint32_t idesc = idesc_bf16(P.nt, GEOM == GEOM_MN);
             // descriptors of stage 0's first sub-block; a descriptor's start-address field is
             // address / 16 in its low bits, so other stages and parts are plain additions
             const uint64_t da0 = GEOM == GEOM_MN ? smem_desc(su32(aring), 1024u, 2048u, kLayoutSW128)
@@ -310,11 +376,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             int ab = 0;
             uint32_t cph = 0;
             bool ok = true;
+            int cur = 0;
             for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                int64_t lt;
+                const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
+                const int kst = pr.kstages;
+                const uint32_t idesc = idesc_bf16(pr.nt, GEOM == GEOM_MN);
+                const uint32_t b_bytes = (uint32_t)pr.nt * kBK * 2;   // one part of one sub-block of B
                 if (!__all_sync(0xffffffffu, mbar_wait(&acc_empty[ab], cph ^ 1, abort_flag, P.wait_ns))) break;
                 tc_fence_after();
-                const uint32_t dcol = tmem_base + (uint32_t)(ab * P.nt);
-                for (int st = 0; st < kstages; ++st) {
+                const uint32_t dcol = tmem_base + (uint32_t)(ab * P.acc_stride);
+                for (int st = 0; st < kst; ++st) {
                     const bool got = mbar_wait(&b_full[bs], bph, abort_flag, P.wait_ns) &&
                                      mbar_wait(&a_conv[as], aph, abort_flag, P.wait_ns);
                     if (!__all_sync(0xffffffffu, got)) {
@@ -322,14 +394,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint64_t da = da0 + ((uint64_t)(as * L.a_bytes) >> 4);
-                    const uint64_t db = db0 + ((uint64_t)(bs * L.bstage_bytes) >> 4);
+                    const uint64_t da = da0 + ((uint64_t)(as * LA.a_bytes) >> 4);
+                    const uint64_t db = db0 + ((uint64_t)(bs * P.bslot) >> 4);
 #pragma unroll
                     for (int sub = 0; sub < kSub; ++sub) {
-                        const uint64_t dahi = da + (uint64_t)((sub * L.asub_bytes) >> 4);
-                        const uint64_t dalo = dahi + (uint64_t)(L.abf_bytes >> 4);
-                        const uint64_t dbhi = db + (uint64_t)((sub * 2 * L.b_bytes) >> 4);
-                        const uint64_t dblo = dbhi + (uint64_t)(L.b_bytes >> 4);
+                        const uint64_t dahi = da + (uint64_t)((sub * LA.asub_bytes) >> 4);
+                        const uint64_t dalo = dahi + (uint64_t)(LA.abf_bytes >> 4);
+                        const uint64_t dbhi = db + (uint64_t)((sub * 2 * b_bytes) >> 4);
+                        const uint64_t dblo = dbhi + (uint64_t)(b_bytes >> 4);
                         mma_bf16(dcol, dahi, dbhi, idesc, (st == 0 && sub == 0) ? 0u : 1u);
                         mma_bf16(dcol, dahi, dblo, idesc, 1u);
                         mma_bf16(dcol, dalo, dbhi, idesc, 1u);
@@ -362,8 +434,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         int64_t n = 0;   // sequence number of the stage across this CTA's tiles
         // Every thread of a group runs every iteration of its residue and reaches the group barrier
         // the same number of times; once the CTA aborts, the waits are skipped and no work is done.
+        int cur = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-            for (int st = 0; st < kstages; ++st, ++n) {
+            int64_t lt;
+            const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
+            const int64_t mper = (pr.inner + kBM - 1) / kBM;
+            for (int st = 0; st < pr.kstages; ++st, ++n) {
                 if ((int)(n % kConvGroups) != g) continue;
                 const int s = (int)(n % AS);
                 const uint32_t ph = (uint32_t)((n / AS) & 1);
@@ -373,11 +449,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll 1
                 for (int sub = 0; sub < kSub; ++sub) {
                     const int kc = st * kSub + sub;
-                    uint8_t* buf = a_at(s) + sub * L.asub_bytes;
+                    uint8_t* buf = a_at(s) + sub * LA.asub_bytes;
                     float4 x[kIters];
                     uint32_t off[kIters];
                     // tile origin for the converters' own loads of A (ldg_a): slice k / first row
-                    const int64_t mt = t % P.tiles_m;
+                    const int64_t mt = lt % pr.tiles_m;
                     const int64_t tk = GEOM == GEOM_MN ? mt / mper : 0;
                     const int64_t r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
 #pragma unroll
@@ -385,33 +461,33 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
                         if (GEOM == GEOM_MN) {
                             const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
-                            if (have && P.ldg_a) {
+                            if (have && pr.ldg_a) {
                                 // elements (l, i .. i+3) of slice tk (of slice tk * KB + row / IB when
                                 // folded), zero outside A
                                 const int64_t gl = (int64_t)kc * kBK + l;
-                                const int64_t sk = P.fold_kb > 1 ? mt * P.fold_kb + ((w * 4) >> P.fold_ib_shift) : tk;
-                                const int64_t i = P.fold_kb > 1 ? ((w * 4) & ((1 << P.fold_ib_shift) - 1)) : r0 + w * 4;
-                                const float* src = P.a + (sk * P.nq + gl) * P.inner + i;
-                                const bool lv = gl < P.nq && sk < P.outer;
-                                x[it].x = (lv && i < P.inner) ? __ldg(src) : 0.0f;
-                                x[it].y = (lv && i + 1 < P.inner) ? __ldg(src + 1) : 0.0f;
-                                x[it].z = (lv && i + 2 < P.inner) ? __ldg(src + 2) : 0.0f;
-                                x[it].w = (lv && i + 3 < P.inner) ? __ldg(src + 3) : 0.0f;
+                                const int64_t sk = pr.fold_kb > 1 ? mt * pr.fold_kb + ((w * 4) >> pr.fold_ib_shift) : tk;
+                                const int64_t i = pr.fold_kb > 1 ? ((w * 4) & ((1 << pr.fold_ib_shift) - 1)) : r0 + w * 4;
+                                const float* src = pr.a + (sk * pr.nq + gl) * pr.inner + i;
+                                const bool lv = gl < pr.nq && sk < pr.outer;
+                                x[it].x = (lv && i < pr.inner) ? __ldg(src) : 0.0f;
+                                x[it].y = (lv && i + 1 < pr.inner) ? __ldg(src + 1) : 0.0f;
+                                x[it].z = (lv && i + 2 < pr.inner) ? __ldg(src + 2) : 0.0f;
+                                x[it].w = (lv && i + 3 < pr.inner) ? __ldg(src + 3) : 0.0f;
                             } else if (have) {
                                 x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
                             }
                             off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
                         } else {
                             const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
-                            if (have && P.ldg_a) {
+                            if (have && pr.ldg_a) {
                                 // elements (row, l .. l+3) of the contiguous fibre row, zero outside A
                                 const int64_t row = r0 + k, gl = (int64_t)kc * kBK + lc * 4;
-                                const float* src = P.a + row * P.nq + gl;
-                                const bool rv = row < P.outer;
-                                x[it].x = (rv && gl < P.nq) ? __ldg(src) : 0.0f;
-                                x[it].y = (rv && gl + 1 < P.nq) ? __ldg(src + 1) : 0.0f;
-                                x[it].z = (rv && gl + 2 < P.nq) ? __ldg(src + 2) : 0.0f;
-                                x[it].w = (rv && gl + 3 < P.nq) ? __ldg(src + 3) : 0.0f;
+                                const float* src = pr.a + row * pr.nq + gl;
+                                const bool rv = row < pr.outer;
+                                x[it].x = (rv && gl < pr.nq) ? __ldg(src) : 0.0f;
+                                x[it].y = (rv && gl + 1 < pr.nq) ? __ldg(src + 1) : 0.0f;
+                                x[it].z = (rv && gl + 2 < pr.nq) ? __ldg(src + 2) : 0.0f;
+                                x[it].w = (rv && gl + 3 < pr.nq) ? __ldg(src + 3) : 0.0f;
                             } else if (have) {
                                 x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
                             }
@@ -431,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
                             const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
                             if (!odd) *reinterpret_cast<uint4*>(buf + off[it]) = pack4(h0, h1, got0, got1);
-                            else *reinterpret_cast<uint4*>(buf + L.abf_bytes + off[it]) = pack4(got0, got1, l0, l1);
+                            else *reinterpret_cast<uint4*>(buf + LA.abf_bytes + off[it]) = pack4(got0, got1, l0, l1);
                         }
                     }
                 }
@@ -450,15 +526,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         int sb = 0;
         int ab = 0;
         uint32_t aph = 0;
+        const TcProb* last = nullptr;
+        int cur = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+            int64_t lt;
+            const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
+            if (GROUP && &pr != last && pr.tma_c) tensormap_acquire(&pr.cmap);
+            last = &pr;
+            const int64_t mper = (pr.inner + kBM - 1) / kBM;
             if (!mbar_wait(&acc_full[ab], aph, abort_flag, P.wait_ns)) break;
             tc_fence_after();
-            const int64_t jb = t / P.tiles_m, mt = t - jb * P.tiles_m;
+            const int64_t jb = lt / pr.tiles_m, mt = lt - jb * pr.tiles_m;
             int64_t k, r0;            // slice and first row (i for GEOM_MN, k for GEOM_K) of this warp
-            if (GEOM == GEOM_MN && P.fold_kb > 1) {
+            if (GEOM == GEOM_MN && pr.fold_kb > 1) {
                 // this warp's 32 rows lie in one slice of the folded tile
-                k = mt * P.fold_kb + ((q4 * 32) >> P.fold_ib_shift);
-                r0 = (q4 * 32) & ((1 << P.fold_ib_shift) - 1);
+                k = mt * pr.fold_kb + ((q4 * 32) >> pr.fold_ib_shift);
+                r0 = (q4 * 32) & ((1 << pr.fold_ib_shift) - 1);
             } else if (GEOM == GEOM_MN) {
                 k = mt / mper;
                 r0 = (mt - k * mper) * kBM + q4 * 32;
@@ -466,17 +549,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                 k = 0;
                 r0 = mt * kBM + q4 * 32;
             }
-            const int64_t jrem = P.m - (int64_t)jb * P.nt;
-            const int jleft = jrem < P.nt ? (int)jrem : P.nt;
-            const uint32_t tbase = tmem_base + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(ab * P.nt);
-            for (int cc = 0; cc < P.nt; cc += 32) {
+            const int nt = pr.nt;
+            const int64_t jrem = pr.m - (int64_t)jb * nt;
+            const int jleft = jrem < nt ? (int)jrem : nt;
+            const uint32_t tbase = tmem_base + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(ab * P.acc_stride);
+            for (int cc = 0; cc < nt; cc += 32) {
                 uint32_t v[32];
                 tmem_ld32(tbase + (uint32_t)cc, v);
                 if (cc >= jleft) continue;
-                const int j0 = jb * P.nt + cc;
-                if (P.tma_c && GEOM == GEOM_MN && k >= P.outer) {
+                const int j0 = jb * nt + cc;
+                if (pr.tma_c && GEOM == GEOM_MN && k >= pr.outer) {
                     // folded last tile: this warp's slice lies past the end of C, nothing to store
-                } else if (P.tma_c) {
+                } else if (pr.tma_c) {
                     // Stage a 32 x 32 block in shared memory and store it with one TMA copy.
                     uint8_t* buf = stage0 + sb * kEpiBuf;
                     if (lane == 0) bulk_wait_read1();      // the copy that last read `buf` has finished reading it
@@ -496,18 +580,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                     fence_proxy_async();
                     __syncwarp();
                     if (lane == 0) {
-                        if (GEOM == GEOM_MN) tma_store_3d(&cmap, buf, (int)r0, j0, (int)k);
-                        else tma_store_2d(&cmap, buf, j0, (int)r0);
+                        if (GEOM == GEOM_MN) tma_store_3d(&pr.cmap, buf, (int)r0, j0, (int)k);
+                        else tma_store_2d(&pr.cmap, buf, j0, (int)r0);
                         bulk_commit();
                     }
                     sb ^= 1;
                 } else {
                     // Direct stores (C rows not 16-byte aligned for a tensor map).
                     const int64_t r = r0 + lane;
-                    const bool rvalid = GEOM == GEOM_MN ? (r < P.inner && k < P.outer) : r < P.outer;
+                    const bool rvalid = GEOM == GEOM_MN ? (r < pr.inner && k < pr.outer) : r < pr.outer;
                     if (rvalid) {
-                        float* p = GEOM == GEOM_MN ? P.c + (k * P.m + j0) * P.inner + r : P.c + r * P.m + j0;
-                        const int64_t cs = GEOM == GEOM_MN ? P.inner : 1;
+                        float* p = GEOM == GEOM_MN ? pr.c + (k * pr.m + j0) * pr.inner + r : pr.c + r * pr.m + j0;
+                        const int64_t cs = GEOM == GEOM_MN ? pr.inner : 1;
 #pragma unroll
                         for (int c = 0; c < 32; ++c)
                             if (cc + c < jleft) p[(int64_t)c * cs] = __uint_as_float(v[c]);
@@ -533,12 +617,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // B (m x nq, column- or row-major FP32) -> bf16 hi/lo images, one per (j block, K chunk),
 // each NT rows x 16 l in the K-major SW32 layout the MMA reads. Zero outside B.
-__global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m, int64_t nq, int nt, int jblocks,
-                               int kchunks, uint8_t* __restrict__ img)
+__device__ __forceinline__ void split_b_units(const float* __restrict__ b, int b_cm, int64_t m, int64_t nq, int nt,
+                                              int jblocks, int kchunks, uint8_t* __restrict__ img, int64_t u0,
+                                              int64_t step)
 {
     const int64_t total = (int64_t)jblocks * kchunks * nt * 2;     // 2 chunks of 8 l per row
     const uint32_t part_bytes = (uint32_t)nt * (kBK * 2);
-    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < total; u += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t u = u0; u < total; u += step) {
         const int c = (int)(u & 1);
         const int64_t rrow = u >> 1;
         const int jl = (int)(rrow % nt);
@@ -562,6 +647,21 @@ __global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m,
         *reinterpret_cast<uint4*>(base + off) = h;
         *reinterpret_cast<uint4*>(base + part_bytes + off) = lo;
     }
+}
+
+__global__ void split_b_kernel(const float* __restrict__ b, int b_cm, int64_t m, int64_t nq, int nt, int jblocks,
+                               int kchunks, uint8_t* __restrict__ img)
+{
+    split_b_units(b, b_cm, m, nq, nt, jblocks, kchunks, img, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                  (int64_t)gridDim.x * blockDim.x);
+}
+
+// The operand split of every problem of a grouped launch: blockIdx.y + y0 is the problem.
+__global__ void split_b_group_kernel(const TcProb* __restrict__ group, int y0)
+{
+    const TcProb& pr = group[blockIdx.y + y0];
+    split_b_units(pr.b, pr.b_cm, pr.m, pr.nq, pr.nt, pr.jblocks, pr.kstages * kSub, const_cast<uint8_t*>(pr.bimg),
+                  (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------------ TMA-fed small-m kernel
@@ -588,7 +688,6 @@ struct StreamParams {
     void* c;
     void* ws;               // S > 1: partial tiles [tiles][S][MB][P]
     unsigned* cnt;          // S > 1: per-tile arrival counters, zero at launch
-    int* status;
     int64_t outer, nq, inner, m;
     int64_t tiles;          // ceil(outer / KB) * mper
     int64_t mper;           // ceil(inner / IB)
@@ -598,11 +697,47 @@ struct StreamParams {
     int kper;               // l chunks per unit
     int S;                  // l ranges per tile
     int b_cm;
-    int stages;             // ring depth, <= kStreamMaxStages
     int ib_shift;           // log2(IB)
     int h_shift;            // log2(H); H > 1 uses the 4D map
     int kb;                 // KB = P / (IB * H)
 };
+
+// One problem of a stream launch: its tensor map and parameters. A single launch passes it as a
+// kernel parameter; a grouped launch reads an array of them from device memory (64-byte aligned).
+struct alignas(64) StreamProb {
+    CUtensorMap amap;
+    StreamParams P;
+    int64_t first;          // grouped launch: index of the problem's first unit among all units
+};
+
+static_assert(sizeof(TcProb) % 64 == 0, "problem records keep their tensor maps 64-byte aligned");
+static_assert(sizeof(StreamProb) % 64 == 0, "problem records keep their tensor maps 64-byte aligned");
+
+// Launch-wide parameters of a stream launch.
+struct StreamLaunch {
+    int* status;
+    const StreamProb* group;   // grouped launch: `count` problems in device memory (else unused)
+    int count;
+    int64_t total;             // units over all problems
+    int stages;                // ring depth, <= kStreamMaxStages
+    int brows;                 // l rows of B the staging area holds (kper * lb of every problem)
+};
+
+// The problem owning unit u of the launch and the unit's index within it; `cur` carries the
+// search on from the previous unit (units are visited in increasing order).
+template <bool GROUP>
+__device__ __forceinline__ const StreamProb& unit_problem(const StreamProb& one, const StreamLaunch& L, int64_t u,
+                                                          int& cur, int64_t& lu)
+{
+    if constexpr (!GROUP) {
+        lu = u;
+        return one;
+    } else {
+        while (cur + 1 < L.count && L.group[cur + 1].first <= u) ++cur;
+        lu = u - L.group[cur].first;
+        return L.group[cur];
+    }
+}
 
 template <typename T> struct V16Tc;
 template <> struct V16Tc<float> { using type = float4; };
@@ -627,20 +762,23 @@ struct StreamGeom {
 // down to 8: 96 for two CTAs (no spills for m <= 8), 168 for one (any m <= 16).
 constexpr int stream_nreg(int cps) { return cps == 2 ? 96 : 168; }
 
-template <typename T, int MB, bool ROWS, int CPS>
+// GROUP = false: one problem, `one`. GROUP = true: the L.count problems of L.group (each with
+// S == 1 and B staged whole), their units numbered one after the other; producer and consumers
+// walk the same unit sequence, so the ring streams across problem boundaries.
+template <typename T, int MB, bool ROWS, int CPS, bool GROUP>
 __global__ void __maxnreg__(stream_nreg(CPS))
-    stream_cols_kernel(const __grid_constant__ CUtensorMap amap, StreamParams P)
+    stream_cols_kernel(const __grid_constant__ StreamProb one, StreamLaunch L)
 {
     using G = StreamGeom<T, ROWS>;
     constexpr int W = G::W, NP = G::P, LB = G::LB;
     using V = typename std::conditional<ROWS, T, typename V16Tc<T>::type>::type;   // W consecutive T
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int stages = P.stages;
+    const int stages = L.stages;
     uint8_t* ring = smem;
     constexpr uint32_t SB = G::SB;
     T* bs = reinterpret_cast<T*>(smem + stages * SB);                          // [kper * lb][MB]
-    uint64_t* full = reinterpret_cast<uint64_t*>(bs + (size_t)P.kper * P.lb * MB);
+    uint64_t* full = reinterpret_cast<uint64_t*>(bs + (size_t)L.brows * MB);
     full = reinterpret_cast<uint64_t*>((reinterpret_cast<uintptr_t>(full) + 15) & ~uintptr_t(15));
     uint64_t* empty = full + kStreamMaxStages;
     volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + kStreamMaxStages);
@@ -658,9 +796,6 @@ __global__ void __maxnreg__(stream_nreg(CPS))
     }
     __syncthreads();
 
-    const int64_t mper = P.mper;
-    const int S = P.S;
-    const int IB = 1 << P.ib_shift;
     if (warp == 8) {
         if (lane == 0) {
             int s = 0;
@@ -668,25 +803,34 @@ __global__ void __maxnreg__(stream_nreg(CPS))
             bool ok = true;
             int issued[kStreamMaxStages];
             for (int i = 0; i < kStreamMaxStages; ++i) issued[i] = -1;
-            for (int64_t u = blockIdx.x; u < P.units && ok; u += gridDim.x) {
-                const int64_t t = u / S;
-                const int r = (int)(u - t * S);
-                const int64_t kb = t / mper, ib = t - kb * mper;
-                const int kc0 = r * P.kper, kc1 = min(kc0 + P.kper, P.kchunks);
+            int cur = 0;
+            const StreamProb* last = nullptr;
+            for (int64_t u = blockIdx.x; u < L.total && ok; u += gridDim.x) {
+                int64_t lu;
+                const StreamProb& pq = unit_problem<GROUP>(one, L, u, cur, lu);
+                if (GROUP && &pq != last) tensormap_acquire(&pq.amap);
+                last = &pq;
+                const StreamParams& Q = pq.P;
+                const int S = Q.S;
+                const int IB = 1 << Q.ib_shift;
+                const int64_t t = lu / S;
+                const int r = (int)(lu - t * S);
+                const int64_t kb = t / Q.mper, ib = t - kb * Q.mper;
+                const int kc0 = r * Q.kper, kc1 = min(kc0 + Q.kper, Q.kchunks);
                 for (int kc = kc0; kc < kc1; ++kc) {
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&full[s], (uint32_t)(NP * P.lb * sizeof(T)));
+                    mbar_expect_tx(&full[s], (uint32_t)(NP * Q.lb * sizeof(T)));
                     if (ROWS) {
-                        tma_load_2d(ring + s * SB, &amap, &full[s], kc * P.lb, (int)(kb * P.kb));
-                        tma_load_2d(ring + s * SB + SB / 2, &amap, &full[s], kc * P.lb,
-                                    (int)(kb * P.kb + 256));
+                        tma_load_2d(ring + s * SB, &pq.amap, &full[s], kc * Q.lb, (int)(kb * Q.kb));
+                        tma_load_2d(ring + s * SB + SB / 2, &pq.amap, &full[s], kc * Q.lb,
+                                    (int)(kb * Q.kb + 256));
                     }
-                    else if (P.h_shift == 0)
-                        tma_load_3d(ring + s * SB, &amap, &full[s], (int)(ib * IB), (int)(kb * P.kb), kc * P.lb);
+                    else if (Q.h_shift == 0)
+                        tma_load_3d(ring + s * SB, &pq.amap, &full[s], (int)(ib * IB), (int)(kb * Q.kb), kc * Q.lb);
                     else
-                        tma_load_4d(ring + s * SB, &amap, &full[s], 0, (int)(ib << P.h_shift), (int)(kb * P.kb),
-                                    kc * P.lb);
+                        tma_load_4d(ring + s * SB, &pq.amap, &full[s], 0, (int)(ib << Q.h_shift), (int)(kb * Q.kb),
+                                    kc * Q.lb);
                     if (++s == stages) { s = 0; ph ^= 1; }
                 }
             }
@@ -699,36 +843,42 @@ __global__ void __maxnreg__(stream_nreg(CPS))
     } else {
         const int tid = threadIdx.x;                       // 0..255
         const int pos = tid * W;                           // first owned position
-        const int kk = pos >> (P.ib_shift + P.h_shift);
-        const int hh = (pos >> P.ib_shift) & ((1 << P.h_shift) - 1), ii = pos & (IB - 1);
-        const T* Bg = static_cast<const T*>(P.b);
-        T* C = static_cast<T*>(P.c);
         int s = 0;
         uint32_t ph = 0;
         bool ok = true;
-        int staged = -1;                                   // l range (r) held in bs
+        int staged = -1, staged_p = -1;                    // l range (r) and problem held in bs
+        int cur = 0;
         // Every consumer runs every iteration and meets the consumer barriers the same number of
         // times; after an abort the waits are skipped and no work is done.
-        for (int64_t u = blockIdx.x; u < P.units; u += gridDim.x) {
-            const int64_t t = u / S;
-            const int r = (int)(u - t * S);
-            const int64_t kb = t / mper, ib = t - kb * mper;
-            const int kc0 = r * P.kper, kc1 = min(kc0 + P.kper, P.kchunks);
-            if (r != staged) {
+        for (int64_t u = blockIdx.x; u < L.total; u += gridDim.x) {
+            int64_t lu;
+            const StreamProb& pq = unit_problem<GROUP>(one, L, u, cur, lu);
+            const StreamParams& Q = pq.P;
+            const int S = Q.S;
+            const int IB = 1 << Q.ib_shift;
+            const int kk = pos >> (Q.ib_shift + Q.h_shift);
+            const int hh = (pos >> Q.ib_shift) & ((1 << Q.h_shift) - 1), ii = pos & (IB - 1);
+            const T* Bg = static_cast<const T*>(Q.b);
+            T* C = static_cast<T*>(Q.c);
+            const int64_t t = lu / S;
+            const int r = (int)(lu - t * S);
+            const int64_t kb = t / Q.mper, ib = t - kb * Q.mper;
+            const int kc0 = r * Q.kper, kc1 = min(kc0 + Q.kper, Q.kchunks);
+            if (r != staged || cur != staged_p) {
                 // stage rows [kc0 * lb, kc1 * lb) of B: bs[l][j] = B(j, l), zero outside B. The
                 // loads go out four at a time ahead of their stores: bs is a generic pointer, so
                 // the compiler would otherwise wait for each load before the next store.
                 asm volatile("bar.sync 1, 256;" ::: "memory");
-                const int total = (kc1 - kc0) * P.lb * MB;
+                const int total = (kc1 - kc0) * Q.lb * MB;
                 for (int e0 = tid; e0 < total; e0 += 256 * 4) {
                     T v[4];
 #pragma unroll
                     for (int x = 0; x < 4; ++x) {
                         const int e = e0 + x * 256;
                         const int lr = e / MB, j = e - lr * MB;
-                        const int64_t l = (int64_t)kc0 * P.lb + lr;
-                        v[x] = (e < total && j < P.m && l < P.nq)
-                                   ? __ldg(P.b_cm ? Bg + j + l * P.m : Bg + j * P.nq + l) : T(0);
+                        const int64_t l = (int64_t)kc0 * Q.lb + lr;
+                        v[x] = (e < total && j < Q.m && l < Q.nq)
+                                   ? __ldg(Q.b_cm ? Bg + j + l * Q.m : Bg + j * Q.nq + l) : T(0);
                     }
 #pragma unroll
                     for (int x = 0; x < 4; ++x)
@@ -736,6 +886,7 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                 }
                 asm volatile("bar.sync 1, 256;" ::: "memory");
                 staged = r;
+                staged_p = cur;
             }
             T acc[W][MB];
 #pragma unroll
@@ -793,8 +944,8 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                     if (lane == 0) mbar_arrive(&empty[s]);
                 } else if (have) {
                     const V* box = reinterpret_cast<const V*>(ring + s * SB) + tid;
-                    const T* brow = bs + (size_t)(kc - kc0) * P.lb * MB;
-                    const int lb = P.lb;
+                    const T* brow = bs + (size_t)(kc - kc0) * Q.lb * MB;
+                    const int lb = Q.lb;
                     // all LB reads up front (the builds for m = 16 run one CTA per SM and have
                     // the registers)
                     V av[LB];
@@ -832,16 +983,16 @@ __global__ void __maxnreg__(stream_nreg(CPS))
             }
             if constexpr (ROWS) {
                 // rows k0 = tile * 512 + tid and k0 + 256; C[k][j] contiguous in j
-                const int64_t kr[2] = {kb * P.kb + tid, kb * P.kb + 256 + tid};
+                const int64_t kr[2] = {kb * Q.kb + tid, kb * Q.kb + 256 + tid};
                 if (S == 1) {
                     if (ok) {
 #pragma unroll
                         for (int w = 0; w < 2; ++w)
-                            if (kr[w] < P.outer) {
-                                T* cp = C + kr[w] * P.m;
+                            if (kr[w] < Q.outer) {
+                                T* cp = C + kr[w] * Q.m;
                                 if constexpr (MB * sizeof(T) % 16 == 0) {
                                     // whole rows of MB outputs on 16-byte boundaries: vector stores
-                                    if (P.m == MB && (reinterpret_cast<uintptr_t>(C) & 15u) == 0) {
+                                    if (Q.m == MB && (reinterpret_cast<uintptr_t>(C) & 15u) == 0) {
                                         using V16 = typename V16Tc<T>::type;
                                         constexpr int EPC = 16 / (int)sizeof(T);
 #pragma unroll
@@ -857,11 +1008,11 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                                 }
 #pragma unroll
                                 for (int j = 0; j < MB; ++j)
-                                    if (j < P.m) cp[j] = acc[w][j];
+                                    if (j < Q.m) cp[j] = acc[w][j];
                             }
                     }
                 } else {
-                    T* wsp = static_cast<T*>(P.ws) + ((size_t)u * MB) * NP;
+                    T* wsp = static_cast<T*>(Q.ws) + ((size_t)lu * MB) * NP;
 #pragma unroll
                     for (int j = 0; j < MB; ++j) {
                         wsp[(size_t)j * NP + tid] = acc[0][j];
@@ -869,16 +1020,16 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                     }
                     __threadfence();
                     asm volatile("bar.sync 1, 256;" ::: "memory");
-                    if (tid == 0) *last_flag = (!*abort_flag && atomicAdd(&P.cnt[t], 1u) == (unsigned)(S - 1)) ? 1 : 0;
+                    if (tid == 0) *last_flag = (!*abort_flag && atomicAdd(&Q.cnt[t], 1u) == (unsigned)(S - 1)) ? 1 : 0;
                     asm volatile("bar.sync 1, 256;" ::: "memory");
                     if (*last_flag) {
                         __threadfence();
-                        const T* w0 = static_cast<const T*>(P.ws) + ((size_t)t * S * MB) * NP;
+                        const T* w0 = static_cast<const T*>(Q.ws) + ((size_t)t * S * MB) * NP;
 #pragma unroll
                         for (int w = 0; w < 2; ++w) {
-                            if (kr[w] >= P.outer) continue;
-                            T* cp = C + kr[w] * P.m;
-                            for (int j = 0; j < MB && j < P.m; ++j) {
+                            if (kr[w] >= Q.outer) continue;
+                            T* cp = C + kr[w] * Q.m;
+                            for (int j = 0; j < MB && j < Q.m; ++j) {
                                 T sum = T(0);
                                 for (int rr = 0; rr < S; ++rr) sum += __ldcg(w0 + ((size_t)rr * MB + j) * NP + w * 256 + tid);
                                 cp[j] = sum;
@@ -888,24 +1039,24 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                 }
                 continue;
             }
-            const int64_t k = kb * P.kb + kk, i = (((ib << P.h_shift) + hh) << P.ib_shift) + ii;
-            const bool mine = k < P.outer && i < P.inner;     // all W positions share k; inner % W == 0
+            const int64_t k = kb * Q.kb + kk, i = (((ib << Q.h_shift) + hh) << Q.ib_shift) + ii;
+            const bool mine = k < Q.outer && i < Q.inner;     // all W positions share k; inner % W == 0
             if (S == 1) {
                 if (ok && mine) {
-                    T* cp = C + (k * P.m) * P.inner + i;
+                    T* cp = C + (k * Q.m) * Q.inner + i;
 #pragma unroll
                     for (int j = 0; j < MB; ++j) {
-                        if (j < P.m) {
+                        if (j < Q.m) {
                             V v;
                             T* vv = reinterpret_cast<T*>(&v);
 #pragma unroll
                             for (int w = 0; w < W; ++w) vv[w] = acc[w][j];
-                            *reinterpret_cast<V*>(cp + (int64_t)j * P.inner) = v;
+                            *reinterpret_cast<V*>(cp + (int64_t)j * Q.inner) = v;
                         }
                     }
                 }
             } else {
-                T* wsp = static_cast<T*>(P.ws) + ((size_t)u * MB) * NP + pos;
+                T* wsp = static_cast<T*>(Q.ws) + ((size_t)lu * MB) * NP + pos;
 #pragma unroll
                 for (int j = 0; j < MB; ++j) {
                     V v;
@@ -916,14 +1067,14 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                 }
                 __threadfence();
                 asm volatile("bar.sync 1, 256;" ::: "memory");
-                if (tid == 0) *last_flag = (!*abort_flag && atomicAdd(&P.cnt[t], 1u) == (unsigned)(S - 1)) ? 1 : 0;
+                if (tid == 0) *last_flag = (!*abort_flag && atomicAdd(&Q.cnt[t], 1u) == (unsigned)(S - 1)) ? 1 : 0;
                 asm volatile("bar.sync 1, 256;" ::: "memory");
                 if (*last_flag) {
                     __threadfence();
                     if (mine) {
-                        const T* w0 = static_cast<const T*>(P.ws) + ((size_t)t * S * MB) * NP + pos;
-                        T* cp = C + (k * P.m) * P.inner + i;
-                        for (int j = 0; j < MB && j < P.m; ++j) {
+                        const T* w0 = static_cast<const T*>(Q.ws) + ((size_t)t * S * MB) * NP + pos;
+                        T* cp = C + (k * Q.m) * Q.inner + i;
+                        for (int j = 0; j < MB && j < Q.m; ++j) {
                             V sum;
                             T* sv = reinterpret_cast<T*>(&sum);
 #pragma unroll
@@ -934,7 +1085,7 @@ __global__ void __maxnreg__(stream_nreg(CPS))
 #pragma unroll
                                 for (int w = 0; w < W; ++w) sv[w] += vv[w];
                             }
-                            *reinterpret_cast<V*>(cp + (int64_t)j * P.inner) = sum;
+                            *reinterpret_cast<V*>(cp + (int64_t)j * Q.inner) = sum;
                         }
                     }
                 }
@@ -942,7 +1093,7 @@ __global__ void __maxnreg__(stream_nreg(CPS))
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && *abort_flag) atomicExch(P.status, 1);
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(L.status, 1);
 }
 
 // ------------------------------------------------------------------ host side
@@ -1080,68 +1231,212 @@ bool tma_a_ok(const View3& v, int geom)
     return geom == GEOM_K ? v.nq % 4 == 0 : v.inner % 4 == 0;
 }
 
+// Fills the problem record of the bf16x3 kernel for view v, its pre-split B image at `img`
+// (tc_image_bytes(v) bytes); *geom receives its geometry.
+void make_tc_prob(const View3& v, uint8_t* img, TcProb& pr, int* geom)
+{
+    std::memset(&pr, 0, sizeof(pr));
+    const int g = geometry_of(v);
+    *geom = g;
+    pr.nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
+    pr.jblocks = (int)((v.m + pr.nt - 1) / pr.nt);
+    pr.kchunks = (int)((v.nq + kBK - 1) / kBK);
+    pr.kstages = (pr.kchunks + kSub - 1) / kSub;
+    pr.ldg_a = tma_a_ok(v, g) ? 0 : 1;
+    pr.a = static_cast<const float*>(v.a);
+    pr.b = static_cast<const float*>(v.b);
+    pr.b_cm = v.b_cm ? 1 : 0;
+    // inner <= 64: KB = 128 / IB slices share a 128-row tile (IB = 32 or 64 rows each)
+    pr.fold_kb = 1;
+    pr.fold_ib_shift = 7;
+    if (g == GEOM_MN && v.inner <= 64) {
+        pr.fold_ib_shift = v.inner <= 32 ? 5 : 6;
+        pr.fold_kb = kBM >> pr.fold_ib_shift;
+    }
+    if (!pr.ldg_a && !(pr.fold_kb > 1 ? encode_a_map_folded(v, 1 << pr.fold_ib_shift, pr.fold_kb, &pr.amap)
+                                      : encode_a_map(v, g, &pr.amap)))
+        pr.ldg_a = 1;   // the driver declined the map: the converters load A
+    if (pr.ldg_a) std::memset(&pr.amap, 0, sizeof(pr.amap));
+    pr.tma_c = encode_c_map(v, g, &pr.cmap) ? 1 : 0;
+    if (!pr.tma_c) std::memset(&pr.cmap, 0, sizeof(pr.cmap));
+    pr.c = static_cast<float*>(v.c);
+    pr.bimg = img;
+    pr.outer = v.outer;
+    pr.nq = v.nq;
+    pr.inner = v.inner;
+    pr.m = v.m;
+    pr.tiles_m = g == GEOM_MN ? (pr.fold_kb > 1 ? (v.outer + pr.fold_kb - 1) / pr.fold_kb
+                                                : v.outer * ((v.inner + kBM - 1) / kBM))
+                              : (v.outer + kBM - 1) / kBM;
+    pr.tiles = pr.tiles_m * pr.jblocks;
+    pr.first = 0;
+}
+
+// Elements of B's image a problem's operand split writes: kstages * kSub sub-blocks of 16 l per
+// j block (zero past n_q), nt rows each, in two 8-l halves.
+int64_t split_units(const TcProb& pr) { return (int64_t)pr.jblocks * (pr.kstages * kSub) * pr.nt * 2; }
+
+template <int GEOM, bool GROUP>
+cudaError_t launch_tc_kernel(const TcProb& one, const TcParams& P, size_t smem, int grid, cudaStream_t s)
+{
+    cudaError_t e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM, GROUP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e == cudaSuccess) tc_bf16x3_kernel<GEOM, GROUP><<<grid, kThreads, smem, s>>>(one, P);
+    return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
 // Splits B into `img` (tc_image_bytes(v) bytes) and launches the bf16x3 kernel for v on stream s.
 cudaError_t run_bf16x3(const View3& v, uint8_t* img, int* status, int sms, cudaStream_t s)
 {
-    const int geom = geometry_of(v);
-    const int nt = (int)std::min<int64_t>(kMaxNT, ((v.m + 15) / 16) * 16);
-    const int jblocks = (int)((v.m + nt - 1) / nt);
-    const int kchunks = (int)((v.nq + kBK - 1) / kBK);
-    const int kstages = (kchunks + kSub - 1) / kSub;
-    CUtensorMap amap, cmap;
+    TcProb pr;
+    int geom = GEOM_MN;
+    make_tc_prob(v, img, pr, &geom);
     TcParams P{};
-    P.ldg_a = tma_a_ok(v, geom) ? 0 : 1;
-    P.a = static_cast<const float*>(v.a);
-    // inner <= 64: KB = 128 / IB slices share a 128-row tile (IB = 32 or 64 rows each)
-    P.fold_kb = 1;
-    P.fold_ib_shift = 7;
-    if (geom == GEOM_MN && v.inner <= 64) {
-        P.fold_ib_shift = v.inner <= 32 ? 5 : 6;
-        P.fold_kb = kBM >> P.fold_ib_shift;
-    }
-    if (!P.ldg_a && !(P.fold_kb > 1 ? encode_a_map_folded(v, 1 << P.fold_ib_shift, P.fold_kb, &amap)
-                                    : encode_a_map(v, geom, &amap)))
-        P.ldg_a = 1;   // the driver declined the map: the converters load A
-    if (P.ldg_a) std::memset(&amap, 0, sizeof(amap));
-    P.tma_c = encode_c_map(v, geom, &cmap) ? 1 : 0;
-    if (!P.tma_c) std::memset(&cmap, 0, sizeof(cmap));
-    P.c = static_cast<float*>(v.c);
-    P.bimg = img;
     P.status = status;
-    P.outer = v.outer;
-    P.nq = v.nq;
-    P.inner = v.inner;
-    P.m = v.m;
-    P.tiles_m = geom == GEOM_MN ? (P.fold_kb > 1 ? (v.outer + P.fold_kb - 1) / P.fold_kb
-                                                 : v.outer * ((v.inner + kBM - 1) / kBM))
-                                : (v.outer + kBM - 1) / kBM;
-    P.tiles = P.tiles_m * jblocks;
-    P.nt = nt;
-    P.jblocks = jblocks;
-    P.kchunks = kchunks;
-    P.kstages = kstages;
+    P.group = nullptr;
+    P.count = 1;
+    P.total = pr.tiles;
+    P.bslot = smem_layout(pr.nt).bstage_bytes;
+    P.acc_stride = pr.nt;
     P.wait_ns = wait_limit_ns();
     P.skip_b = take_skip_b() ? 1 : 0;
     size_t smem = 0;
-    if (!choose_stages(nt, P.fstages, P.ostages, smem)) return cudaErrorNotSupported;
+    if (!choose_stages(pr.nt, P.fstages, P.ostages, smem)) return cudaErrorNotSupported;
 
-    // the image holds kstages * kSub sub-blocks per j block (zero past n_q)
-    const int64_t total = (int64_t)jblocks * (kstages * kSub) * nt * 2;
+    const int64_t total = split_units(pr);
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-    split_b_kernel<<<blocks, 256, 0, s>>>(static_cast<const float*>(v.b), v.b_cm, v.m, v.nq, nt, jblocks,
-                                          kstages * kSub, img);
+    split_b_kernel<<<blocks, 256, 0, s>>>(pr.b, pr.b_cm, pr.m, pr.nq, pr.nt, pr.jblocks, pr.kstages * kSub, img);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const int grid = (int)std::min<int64_t>(P.tiles, sms);
-    if (geom == GEOM_MN) {
-        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_MN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_MN><<<grid, kThreads, smem, s>>>(amap, cmap, P);
-    } else {
-        e = cudaFuncSetAttribute(tc_bf16x3_kernel<GEOM_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) tc_bf16x3_kernel<GEOM_K><<<grid, kThreads, smem, s>>>(amap, cmap, P);
-    }
-    return e == cudaSuccess ? cudaGetLastError() : e;
+    const int grid = (int)std::min<int64_t>(pr.tiles, sms);
+    return geom == GEOM_MN ? launch_tc_kernel<GEOM_MN, false>(pr, P, smem, grid, s)
+                           : launch_tc_kernel<GEOM_K, false>(pr, P, smem, grid, s);
 }
+
+}  // namespace
+
+// ------------------------------------------------------------------ grouped bf16x3 launch
+struct TcGroup {
+    TcProb* d_probs = nullptr;    // device records: the GEOM_MN problems, then the GEOM_K ones
+    uint8_t* d_img = nullptr;     // all pre-split B images
+    int* status = nullptr;
+    int count = 0;
+    int split_x = 1;              // blocks per problem of the operand split
+    TcParams P[2] = {};           // per geometry (count 0: none)
+    size_t smem[2] = {0, 0};
+    int grid[2] = {0, 0};
+};
+
+namespace {
+const TcProb g_no_prob{};        // the unused single-problem parameter of grouped launches
+}
+
+cudaError_t tc_group_create(const View3* views, int count, TcGroup** out)
+{
+    *out = nullptr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    DevState* st = nullptr;
+    if ((e = state_for(dev, st)) != cudaSuccess) return e;
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    std::unique_ptr<TcGroup, void (*)(TcGroup*)> G(new TcGroup(), tc_group_destroy);
+    G->status = st->status;
+    G->count = count;
+    if (count == 0) {
+        *out = G.release();
+        return cudaSuccess;
+    }
+    std::vector<size_t> img_off(count);
+    size_t img_total = 0;
+    for (int i = 0; i < count; ++i) {
+        img_off[i] = img_total;
+        img_total += (tc_image_bytes(views[i]) + 255) & ~size_t(255);
+    }
+    if ((e = dev_malloc(reinterpret_cast<void**>(&G->d_img), img_total)) != cudaSuccess) return e;
+    std::vector<TcProb> probs(count);
+    std::vector<int> geom(count);
+    for (int i = 0; i < count; ++i) make_tc_prob(views[i], G->d_img + img_off[i], probs[i], &geom[i]);
+    // GEOM_MN first, then GEOM_K; within each, the problems with the heaviest tiles first, so
+    // that the round robin of tiles over the persistent CTAs ends on light ones
+    std::vector<int> order(count);
+    for (int i = 0; i < count; ++i) order[i] = i;
+    auto tile_cost = [&](int i) { return (int64_t)probs[i].kstages * probs[i].nt; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (geom[x] != geom[y]) return geom[x] < geom[y];
+        return tile_cost(x) > tile_cost(y);
+    });
+    std::vector<TcProb> sorted(count);
+    int64_t first[2] = {0, 0};
+    int ntmax[2] = {16, 16}, n[2] = {0, 0};
+    int64_t max_units = 0;
+    for (int r = 0; r < count; ++r) {
+        const int i = order[r], g = geom[i];
+        sorted[r] = probs[i];
+        sorted[r].first = first[g];
+        first[g] += probs[i].tiles;
+        ntmax[g] = std::max(ntmax[g], probs[i].nt);
+        ++n[g];
+        max_units = std::max(max_units, split_units(probs[i]));
+    }
+    if ((e = dev_malloc(reinterpret_cast<void**>(&G->d_probs), sizeof(TcProb) * count)) != cudaSuccess) return e;
+    if ((e = cudaMemcpy(G->d_probs, sorted.data(), sizeof(TcProb) * count, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    G->split_x = (int)std::max<int64_t>(1, std::min<int64_t>((max_units + 255) / 256, 64));
+    for (int g = 0; g < 2; ++g) {
+        TcParams& P = G->P[g];
+        P = TcParams{};
+        P.count = n[g];
+        if (n[g] == 0) continue;
+        P.status = G->status;
+        P.group = G->d_probs + (g == 0 ? 0 : n[0]);
+        P.total = first[g];
+        P.bslot = smem_layout(ntmax[g]).bstage_bytes;
+        P.acc_stride = ntmax[g];
+        if (!choose_stages(ntmax[g], P.fstages, P.ostages, G->smem[g])) return cudaErrorNotSupported;
+        G->grid[g] = (int)std::min<int64_t>(P.total, sms);
+    }
+    *out = G.release();
+    return cudaSuccess;
+}
+
+cudaError_t tc_group_run(TcGroup* G, cudaStream_t s)
+{
+    if (!G || G->count == 0) return cudaSuccess;
+    for (int y0 = 0; y0 < G->count; y0 += 65535) {
+        const int ny = std::min(G->count - y0, 65535);
+        split_b_group_kernel<<<dim3((unsigned)G->split_x, (unsigned)ny), 256, 0, s>>>(G->d_probs, y0);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    for (int g = 0; g < 2; ++g) {
+        TcParams P = G->P[g];
+        if (P.count == 0) continue;
+        P.wait_ns = wait_limit_ns();
+        P.skip_b = take_skip_b() ? 1 : 0;
+        cudaError_t e = g == 0 ? launch_tc_kernel<GEOM_MN, true>(g_no_prob, P, G->smem[g], G->grid[g], s)
+                               : launch_tc_kernel<GEOM_K, true>(g_no_prob, P, G->smem[g], G->grid[g], s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+int tc_group_launches(const TcGroup* G)
+{
+    if (!G || G->count == 0) return 0;
+    return (G->count + 65534) / 65535 + (G->P[0].count > 0) + (G->P[1].count > 0);
+}
+
+void tc_group_destroy(TcGroup* G)
+{
+    if (!G) return;
+    if (G->d_probs) cudaFree(G->d_probs);
+    if (G->d_img) cudaFree(G->d_img);
+    delete G;
+}
+
+namespace {
 
 // A as a tensor map over (i, k, l), or with h > 1 over (i mod ib, i / ib, k, l) (ib must divide
 // inner) -- dimensions deliberately not in stride order -- with boxes of ib x [h x] kb x LB.
@@ -1190,38 +1485,49 @@ cudaError_t allow_smem_once(K kernel, int dev, std::atomic<uint64_t>& done, bool
     return e;
 }
 
-template <typename T, int MB, bool ROWS, int CPS>
-cudaError_t launch_stream_mb(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
+template <typename T, int MB, bool ROWS, int CPS, bool GROUP>
+cudaError_t launch_stream_mb(const StreamProb& one, const StreamLaunch& L, size_t smem, int grid, int dev,
                              cudaStream_t s)
 {
     static std::atomic<uint64_t> done{0};
     // the whole unified L1 as shared memory, so that CPS rings fit side by side
-    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS, CPS>, dev, done, true);
+    cudaError_t e = allow_smem_once(stream_cols_kernel<T, MB, ROWS, CPS, GROUP>, dev, done, true);
     if (e != cudaSuccess) return e;
-    stream_cols_kernel<T, MB, ROWS, CPS><<<grid, kStreamThreads, smem, s>>>(amap, P);
+    stream_cols_kernel<T, MB, ROWS, CPS, GROUP><<<grid, kStreamThreads, smem, s>>>(one, L);
     return cudaGetLastError();
 }
 
 // The build for `cps` CTAs per SM: two for m <= 8, one for any m.
-template <typename T, int MB, bool ROWS>
-cudaError_t launch_stream_cps(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
-                              int cps, cudaStream_t s)
+template <typename T, int MB, bool ROWS, bool GROUP>
+cudaError_t launch_stream_cps(const StreamProb& one, const StreamLaunch& L, size_t smem, int grid, int dev, int cps,
+                              cudaStream_t s)
 {
     if constexpr (MB <= 8) {
-        if (cps == 2) return launch_stream_mb<T, MB, ROWS, 2>(amap, P, smem, grid, dev, s);
+        if (cps == 2) return launch_stream_mb<T, MB, ROWS, 2, GROUP>(one, L, smem, grid, dev, s);
     }
-    return launch_stream_mb<T, MB, ROWS, 1>(amap, P, smem, grid, dev, s);
+    return launch_stream_mb<T, MB, ROWS, 1, GROUP>(one, L, smem, grid, dev, s);
 }
 
-template <typename T, bool ROWS>
-cudaError_t launch_stream_t(const CUtensorMap& amap, const StreamParams& P, size_t smem, int grid, int dev,
+// `mb`: the MB build (1, 2, 4, 8 or 16) covering every m of the launch.
+template <typename T, bool ROWS, bool GROUP>
+cudaError_t launch_stream_t(const StreamProb& one, const StreamLaunch& L, int mb, size_t smem, int grid, int dev,
                             int cps, cudaStream_t s)
 {
-    if (P.m <= 1) return launch_stream_cps<T, 1, ROWS>(amap, P, smem, grid, dev, cps, s);
-    if (P.m <= 2) return launch_stream_cps<T, 2, ROWS>(amap, P, smem, grid, dev, cps, s);
-    if (P.m <= 4) return launch_stream_cps<T, 4, ROWS>(amap, P, smem, grid, dev, cps, s);
-    if (P.m <= 8) return launch_stream_cps<T, 8, ROWS>(amap, P, smem, grid, dev, cps, s);
-    return launch_stream_cps<T, 16, ROWS>(amap, P, smem, grid, dev, cps, s);
+    if (mb <= 1) return launch_stream_cps<T, 1, ROWS, GROUP>(one, L, smem, grid, dev, cps, s);
+    if (mb <= 2) return launch_stream_cps<T, 2, ROWS, GROUP>(one, L, smem, grid, dev, cps, s);
+    if (mb <= 4) return launch_stream_cps<T, 4, ROWS, GROUP>(one, L, smem, grid, dev, cps, s);
+    if (mb <= 8) return launch_stream_cps<T, 8, ROWS, GROUP>(one, L, smem, grid, dev, cps, s);
+    return launch_stream_cps<T, 16, ROWS, GROUP>(one, L, smem, grid, dev, cps, s);
+}
+
+template <bool GROUP>
+cudaError_t launch_stream_any(const StreamProb& one, const StreamLaunch& L, int dtype, bool rows, int mb, size_t smem,
+                              int grid, int dev, int cps, cudaStream_t s)
+{
+    return rows ? (dtype == 0 ? launch_stream_t<float, true, GROUP>(one, L, mb, smem, grid, dev, cps, s)
+                              : launch_stream_t<double, true, GROUP>(one, L, mb, smem, grid, dev, cps, s))
+                : (dtype == 0 ? launch_stream_t<float, false, GROUP>(one, L, mb, smem, grid, dev, cps, s)
+                              : launch_stream_t<double, false, GROUP>(one, L, mb, smem, grid, dev, cps, s));
 }
 
 // Row mode: A as the 2-D tensor map (l, row) of its contiguous fibres, boxes of LB l (64 bytes) x
@@ -1400,6 +1706,29 @@ bool permuted_maps_ok()
     return ok;
 }
 
+// The per-problem parameters of the stream kernel for view v with shape sh (no workspace).
+void fill_stream_params(const View3& v, const StreamShape& sh, StreamParams& P)
+{
+    P = StreamParams{};
+    P.b = v.b;
+    P.c = v.c;
+    P.outer = v.outer;
+    P.nq = v.nq;
+    P.inner = v.inner;
+    P.m = v.m;
+    P.tiles = sh.tiles;
+    P.mper = sh.mper;
+    P.units = sh.units;
+    P.kchunks = sh.kchunks;
+    P.lb = sh.lb;
+    P.kper = sh.kper;
+    P.S = sh.S;
+    P.b_cm = v.b_cm;
+    P.ib_shift = sh.ib_shift;
+    P.h_shift = sh.h_shift;
+    P.kb = sh.kb;
+}
+
 bool stream_supported(const View3& v, int dtype)
 {
     const int64_t w = dtype == 0 ? 4 : 2;
@@ -1432,47 +1761,167 @@ cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s)
     if ((e = state_for(dev, st)) != cudaSuccess) return e;
     StreamShape sh;
     if (!stream_shape(v, dtype, g_sm_count, sh)) return cudaErrorNotSupported;
-    CUtensorMap amap;
-    if (sh.rows ? !encode_rows_map(v, dtype, &amap) : !encode_stream_map(v, dtype, sh.ib, 1 << sh.h_shift, sh.kb, &amap))
+    StreamProb one;
+    std::memset(&one, 0, sizeof(one));
+    if (sh.rows ? !encode_rows_map(v, dtype, &one.amap)
+                : !encode_stream_map(v, dtype, sh.ib, 1 << sh.h_shift, sh.kb, &one.amap))
         return cudaErrorInvalidValue;
-    StreamParams P{};
-    P.b = v.b;
-    P.c = v.c;
-    P.status = st->status;
-    P.outer = v.outer;
-    P.nq = v.nq;
-    P.inner = v.inner;
-    P.m = v.m;
-    P.tiles = sh.tiles;
-    P.mper = sh.mper;
-    P.units = sh.units;
-    P.kchunks = sh.kchunks;
-    P.lb = sh.lb;
-    P.kper = sh.kper;
-    P.S = sh.S;
-    P.b_cm = v.b_cm;
-    P.stages = sh.stages;
-    P.ib_shift = sh.ib_shift;
-    P.h_shift = sh.h_shift;
-    P.kb = sh.kb;
+    fill_stream_params(v, sh, one.P);
+    StreamLaunch L{};
+    L.status = st->status;
+    L.count = 1;
+    L.total = sh.units;
+    L.stages = sh.stages;
+    L.brows = sh.kper * sh.lb;
     void* scratch = nullptr;
     if (sh.S > 1) {
         const size_t ws = (sh.ws_bytes + 255) & ~size_t(255);
         if ((e = dev_malloc_async(&scratch, ws + (size_t)sh.tiles * sizeof(unsigned), s)) != cudaSuccess) return e;
-        P.ws = scratch;
-        P.cnt = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(scratch) + ws);
-        e = cudaMemsetAsync(P.cnt, 0, (size_t)sh.tiles * sizeof(unsigned), s);
+        one.P.ws = scratch;
+        one.P.cnt = reinterpret_cast<unsigned*>(static_cast<uint8_t*>(scratch) + ws);
+        e = cudaMemsetAsync(one.P.cnt, 0, (size_t)sh.tiles * sizeof(unsigned), s);
     }
     const int grid = (int)std::min<int64_t>(sh.units, (int64_t)g_sm_count * sh.per_sm);
-    if (e == cudaSuccess) {
-        const int cps = sh.per_sm;
-        e = sh.rows ? (dtype == 0 ? launch_stream_t<float, true>(amap, P, sh.smem, grid, dev, cps, s)
-                                  : launch_stream_t<double, true>(amap, P, sh.smem, grid, dev, cps, s))
-                    : (dtype == 0 ? launch_stream_t<float, false>(amap, P, sh.smem, grid, dev, cps, s)
-                                  : launch_stream_t<double, false>(amap, P, sh.smem, grid, dev, cps, s));
-    }
+    if (e == cudaSuccess)
+        e = launch_stream_any<false>(one, L, dtype, sh.rows, sh.mb, sh.smem, grid, dev, sh.per_sm, s);
     if (scratch) cudaFreeAsync(scratch, s);
     return e;
+}
+
+// ------------------------------------------------------------------ grouped stream launch
+struct StreamGroup {
+    struct Cls {
+        bool rows;
+        int mb, cps, grid;
+        size_t smem;
+        StreamLaunch L;
+    };
+    StreamProb* d_probs = nullptr;   // the problems of every class, class after class
+    int dtype = 0;
+    std::vector<Cls> cls;
+};
+
+namespace {
+const StreamProb g_no_sprob{};      // the unused single-problem parameter of grouped launches
+
+int group_cps(const StreamShape& sh) { return (sh.rows || sh.mb > 8) ? 1 : 2; }
+size_t group_budget(int cps) { return (size_t)(cps == 2 ? 112 : 227) * 1024; }
+size_t group_smem(const StreamShape& sh, int stages, int brows, size_t es)
+{
+    return 1024 + (size_t)stages * sh.sb + (size_t)brows * sh.mb * es + 256;
+}
+}  // namespace
+
+bool stream_group_eligible(const View3& v, int dtype)
+{
+    if (!stream_supported(v, dtype)) return false;
+    StreamShape sh;
+    if (!stream_shape(v, dtype, 148, sh)) return false;
+    // B staged whole (no l split) beside a ring of at least two stages
+    return group_smem(sh, 2, sh.kchunks * sh.lb, dtype == 0 ? 4 : 8) <= group_budget(group_cps(sh));
+}
+
+cudaError_t stream_group_create(const View3* views, int count, int dtype, StreamGroup** out)
+{
+    *out = nullptr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    DevState* st = nullptr;
+    if ((e = state_for(dev, st)) != cudaSuccess) return e;
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    std::unique_ptr<StreamGroup, void (*)(StreamGroup*)> G(new StreamGroup(), stream_group_destroy);
+    G->dtype = dtype;
+    const size_t es = dtype == 0 ? 4 : 8;
+    // classes by (row mode, MB build, CTAs per SM): one launch each
+    struct Entry { int key; StreamShape sh; int i; };
+    std::vector<Entry> ents;
+    for (int i = 0; i < count; ++i) {
+        StreamShape sh;
+        if (!stream_shape(views[i], dtype, sms, sh)) return cudaErrorNotSupported;
+        sh.kper = sh.kchunks;   // B staged whole: one unit per tile
+        sh.S = 1;
+        sh.units = sh.tiles;
+        const int cps = group_cps(sh);
+        if (group_smem(sh, 2, sh.kchunks * sh.lb, es) > group_budget(cps)) return cudaErrorNotSupported;
+        ents.push_back(Entry{(sh.rows ? 100 : 0) + sh.mb * 4 + cps, sh, i});
+    }
+    std::stable_sort(ents.begin(), ents.end(), [](const Entry& x, const Entry& y) {
+        if (x.key != y.key) return x.key < y.key;
+        return x.sh.units > y.sh.units;
+    });
+    std::vector<StreamProb> recs(ents.size());
+    for (size_t r = 0; r < ents.size();) {
+        size_t r1 = r;
+        int brows = 0;
+        int64_t first = 0;
+        while (r1 < ents.size() && ents[r1].key == ents[r].key) {
+            const Entry& en = ents[r1];
+            StreamProb& pr = recs[r1];
+            std::memset(&pr, 0, sizeof(pr));
+            const View3& v = views[en.i];
+            if (en.sh.rows ? !encode_rows_map(v, dtype, &pr.amap)
+                           : !encode_stream_map(v, dtype, en.sh.ib, 1 << en.sh.h_shift, en.sh.kb, &pr.amap))
+                return cudaErrorInvalidValue;
+            fill_stream_params(v, en.sh, pr.P);
+            pr.first = first;
+            first += en.sh.units;
+            brows = std::max(brows, en.sh.kchunks * en.sh.lb);
+            ++r1;
+        }
+        const StreamShape& sh = ents[r].sh;
+        StreamGroup::Cls c{};
+        c.rows = sh.rows;
+        c.mb = sh.mb;
+        c.cps = group_cps(sh);
+        // the ring of the single launches (128 KB, or 48 KB at two CTAs per SM), less while B
+        // does not fit beside it
+        int stages = std::min<int>(kStreamMaxStages, (int)((c.cps == 2 ? 48 : 128) * 1024 / sh.sb));
+        while (stages > 2 && group_smem(sh, stages, brows, es) > group_budget(c.cps)) --stages;
+        c.smem = group_smem(sh, stages, brows, es);
+        c.L.status = st->status;
+        c.L.count = (int)(r1 - r);
+        c.L.total = first;
+        c.L.stages = stages;
+        c.L.brows = brows;
+        c.L.group = reinterpret_cast<const StreamProb*>(r);   // index for now; a pointer after the upload
+        c.grid = (int)std::min<int64_t>(first, (int64_t)sms * c.cps);
+        G->cls.push_back(c);
+        r = r1;
+    }
+    if (!recs.empty()) {
+        if ((e = dev_malloc(reinterpret_cast<void**>(&G->d_probs), sizeof(StreamProb) * recs.size())) != cudaSuccess)
+            return e;
+        if ((e = cudaMemcpy(G->d_probs, recs.data(), sizeof(StreamProb) * recs.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return e;
+    }
+    for (StreamGroup::Cls& c : G->cls) c.L.group = G->d_probs + reinterpret_cast<uintptr_t>(c.L.group);
+    *out = G.release();
+    return cudaSuccess;
+}
+
+cudaError_t stream_group_run(StreamGroup* G, cudaStream_t s)
+{
+    if (!G) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    for (const StreamGroup::Cls& c : G->cls)
+        if ((e = launch_stream_any<true>(g_no_sprob, c.L, G->dtype, c.rows, c.mb, c.smem, c.grid, dev, c.cps, s)) !=
+            cudaSuccess)
+            return e;
+    return cudaSuccess;
+}
+
+int stream_group_launches(const StreamGroup* G) { return G ? (int)G->cls.size() : 0; }
+
+void stream_group_destroy(StreamGroup* G)
+{
+    if (!G) return;
+    if (G->d_probs) cudaFree(G->d_probs);
+    delete G;
 }
 
 cudaError_t tc_status_word(int dev, int** out)

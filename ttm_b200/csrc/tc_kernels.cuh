@@ -25,6 +25,16 @@ cudaError_t launch_tc_single(const View3& v, cudaStream_t s, int* kid);
 bool tc_pair_supported(const View3& v);
 cudaError_t launch_tc_pair(const View3& v, int* status, cudaStream_t s);
 
+// A grouped bf16x3 launch: many float problems (each with tc_supported) whose tiles are
+// numbered one after the other and run by one persistent launch per geometry (rows of i, or
+// contiguous fibres), after one operand-split launch for all their B. Created once (tensor
+// maps, B images and the problem records in device memory); each run reads the same buffers.
+struct TcGroup;
+cudaError_t tc_group_create(const View3* views, int count, TcGroup** out);
+cudaError_t tc_group_run(TcGroup* g, cudaStream_t s);
+int tc_group_launches(const TcGroup* g);   // kernel launches per run
+void tc_group_destroy(TcGroup* g);
+
 // Creates the per-device state of the tensor-core paths ahead of time (so that a later stream
 // capture does not need to allocate it).
 cudaError_t tc_prepare_device();
@@ -32,6 +42,17 @@ cudaError_t tc_prepare_device();
 // TMA-fed exact small-m kernel for strided fibres (inner % 4 == 0, m <= 16, B fits shared memory).
 bool stream_supported(const View3& v, int dtype);
 cudaError_t launch_stream(const View3& v, int dtype, cudaStream_t s);
+
+// A grouped stream launch: many small-m problems (each with stream_group_eligible: the stream
+// kernel takes it with B staged whole) whose units are numbered one after the other and run by one
+// persistent launch per (row or column mode, MB build, CTAs per SM) class. Created once (tensor
+// maps and problem records in device memory); each run reads the same buffers.
+struct StreamGroup;
+bool stream_group_eligible(const View3& v, int dtype);
+cudaError_t stream_group_create(const View3* views, int count, int dtype, StreamGroup** out);
+cudaError_t stream_group_run(StreamGroup* g, cudaStream_t s);
+int stream_group_launches(const StreamGroup* g);   // kernel launches per run
+void stream_group_destroy(StreamGroup* g);
 
 // Frees device state owned by the tensor-core paths on the current device.
 void tc_release_buffers();

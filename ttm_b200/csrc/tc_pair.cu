@@ -615,9 +615,15 @@ cudaError_t launch_tc_pair(const View3& v, int* status, cudaStream_t s)
     CUtensorMap cmap;
     P.tma_c = encode_pair_cmap(v, geom, &cmap) ? 1 : 0;
     if (!P.tma_c) std::memset(&cmap, 0, sizeof(cmap));
-    // A ring: as many 8 KB stages as fit beside the epilogue staging and the barriers
+    // A ring: as many stages as fit beside the epilogue staging and the barriers, a multiple of
+    // the converter groups. Group g converts the stages n = g (mod groups) in order, waiting on
+    // the stage's barrier by phase parity; with the ring a multiple of the groups every slot
+    // belongs to one group, which sees each phase of it in turn. Otherwise a group could wait on
+    // a slot whose previous load (another group's) has not landed yet, and the parity of that
+    // pending phase would read as the completed one before it.
     const size_t avail = 227 * 1024 - 1024 - kEpiBytesP - kCtrlBytesP;
     P.stages = (int)std::min<size_t>(kMaxStagesP, avail / kStageBytes);
+    P.stages -= P.stages % kConvGroupsP;
     const size_t smem = 1024 + (size_t)P.stages * kStageBytes + kEpiBytesP + kCtrlBytesP;
     return geom == PGEOM_MN ? launch_pair_geom<PGEOM_MN>(amap, cmap, P, smem, dev, s)
                             : launch_pair_geom<PGEOM_K>(amap, cmap, P, smem, dev, s);

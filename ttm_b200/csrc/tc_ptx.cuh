@@ -45,6 +45,22 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase)
     return ok != 0;
 }
 
+// try_wait with a suspend-time hint: the thread sleeps until the phase completes or about
+// `hint_ns` have passed, instead of polling (polling warps take issue slots from the warps doing
+// the work on the same scheduler).
+__device__ __forceinline__ bool mbar_try_sleep(uint64_t* bar, uint32_t phase, uint32_t hint_ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(bar)), "r"(phase), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr uint32_t kSleepHintNs = 20000;   // re-checks of the abort flag and the bound: every ~20 us
+
 // Bounded wait: false when the CTA is aborting or this wait expired (which starts the abort).
 // `limit_ns` is the bound (kernels that take it as a launch parameter let a test shorten it).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag,
@@ -53,7 +69,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatil
     if (mbar_try(bar, phase)) return true;
     const unsigned long long t0 = gtimer();
     while (true) {
-        if (mbar_try(bar, phase)) return true;
+        if (mbar_try_sleep(bar, phase, kSleepHintNs)) return true;
         if (*abort_flag) return false;
         if (gtimer() - t0 > limit_ns) {
             *abort_flag = 1;
