@@ -232,8 +232,9 @@ int tlibttm_plan_run(tlibttm_plan* plan, void* stream);
 /*
  * Runs the plan as a CUDA graph: the first call captures the plan's launches
  * into a graph and instantiates it, later calls replay it (one launch of the
- * whole plan). With stream == NULL a stream owned by the plan is used and the
- * call waits for completion.
+ * whole plan). With stream == NULL a blocking stream owned by the plan is used
+ * (ordered after the work queued on the legacy default stream before the call,
+ * as the default stream itself would be) and the call waits for completion.
  */
 int tlibttm_plan_run_graph(tlibttm_plan* plan, void* stream);
 

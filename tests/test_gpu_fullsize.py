@@ -138,6 +138,13 @@ def test_tucker_192_chain_multilinear_identity(cuda):
     chain.run_graph()
     torch.cuda.synchronize()
     chain.close()
+    # the whole chain in FP64 on the device (first-order memory: index [i4][i3][i2][i1])
+    X = A.view(S, S, S, S).double()
+    for spec, u in zip(["dcba,ja->dcbj", "dcbj,kb->dckj", "dckj,lc->dlkj", "dlkj,md->mlkj"], Us):
+        X = torch.einsum(spec, X, u.double())
+    err = ((Cc.view(r, r, r, r).double() - X).norm() / X.norm()).item()
+    del X
+    assert err <= 2e-5, err                                    # four bf16x3 steps of ~4.5e-6 each
     C4 = Cc.double().cpu().numpy().reshape(r, r, r, r)         # first-order: [j4][j3][j2][j1]
     U = [u.double().cpu().numpy() for u in Us]
     rng = np.random.default_rng(5)

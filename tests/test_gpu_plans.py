@@ -222,3 +222,27 @@ def test_grouped_small_m_launch(cuda, dt):
             pr["A"].mul_(1.5)
             pr["B"].sub_(0.25)
     plan.close()
+
+
+def test_graph_replay_without_a_stream_waits_for_queued_work(cuda):
+    """run_graph() on the default stream replays on a stream the plan owns; that stream must start
+    after the work already queued on the default stream (here: the kernels writing new inputs),
+    exactly as a launch on the default stream itself would."""
+    import torch
+    from ttm_b200.plans import BatchPlan
+    probs = _random_problems(cuda, 12, torch.float32, seed=21)
+    a0 = [pr["A"].clone() for pr in probs]
+    plan = BatchPlan(probs, precision="plain")
+    plan.run_graph()
+    torch.cuda.synchronize()
+    c0 = [pr["C"].clone() for pr in probs]
+    for rnd in range(3):
+        for pr, a in zip(probs, a0):
+            pr["A"].zero_()
+            for _ in range(16):           # many queued kernels before the replay
+                pr["A"].add_(a, alpha=1.0 / 16)
+        plan.run_graph()                  # no synchronisation in between
+        torch.cuda.synchronize()
+        for pr, c in zip(probs, c0):
+            assert torch.allclose(pr["C"], c, rtol=1e-5, atol=1e-5), rnd
+    plan.close()

@@ -580,6 +580,8 @@ int run(const Args& x, int precision, void* stream)
 // specialised kernels beat the grouped launch's generic tiles well below the single-call
 // threshold above.
 constexpr int64_t kPlanSingleMinElems = int64_t(1) << 18;
+// Small-m problems the TMA-fed kernel does not take run on their own from this size
+constexpr int64_t kPlanSmallSingleMinElems = int64_t(1) << 22;
 constexpr int kPlanStreams = 4;     // worker streams the singles of a batched plan spread over
 
 struct Single {            // one problem launched on its own inside a plan
@@ -638,10 +640,13 @@ struct tlibttm_plan_s {
     int dtype = 0, precision = 0, dev = 0;
     // batched
     std::vector<tlibttm::GroupDesc> descs;
-    tlibttm::GroupDesc* d_desc = nullptr;
-    unsigned long long* d_queue = nullptr;
-    int64_t total = 0;
+    tlibttm::GroupDesc* d_desc = nullptr;   // slice-GEMM problems, then small-m problems
+    unsigned long long* d_queue = nullptr;   // [2]: work counters of the two grouped launches
+    int64_t total = 0;                       // slice-GEMM work items
     int grid = 0;
+    int n_small = 0;                         // small-m problems (the last descriptors)
+    int64_t stotal = 0;                      // their work items
+    int sgrid = 0;
     std::vector<tlibttm::Single> singles;   // individual launches (batched extras, or chain steps)
     tlibttm::TcGroup* tcg = nullptr;         // batched: the grouped bf16x3 launch
     tlibttm::StreamGroup* sg = nullptr;      // batched: the grouped small-m launch
@@ -691,10 +696,16 @@ int plan_run_impl(tlibttm_plan* P, cudaStream_t s)
         if ((rc = note_launch(stream_group_run(P->sg, s), K_STREAM_COLS))) return rc;
         g_launches += (unsigned long long)(stream_group_launches(P->sg) - 1);
     }
-    if (P->type == 0 && P->total > 0) {
-        e = cudaMemsetAsync(P->d_queue, 0, sizeof(unsigned long long), s);
+    if (P->type == 0 && !P->descs.empty()) {
+        e = cudaMemsetAsync(P->d_queue, 0, 2 * sizeof(unsigned long long), s);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-        if ((rc = note_launch(launch_grouped(P->d_desc, (int)P->descs.size(), P->total, P->d_queue, P->dtype, P->grid, s),
+        const int n_gemm = (int)P->descs.size() - P->n_small;
+        if (P->total > 0 &&
+            (rc = note_launch(launch_grouped(P->d_desc, n_gemm, P->total, P->d_queue, P->dtype, P->grid, s), K_GROUPED)))
+            return rc;
+        if (P->stotal > 0 &&
+            (rc = note_launch(launch_grouped_small(P->d_desc + n_gemm, P->n_small, P->stotal, P->d_queue + 1, P->dtype,
+                                                   P->sgrid, s),
                               K_GROUPED)))
             return rc;
     }
@@ -732,6 +743,8 @@ void plan_free(tlibttm_plan* P)
 }
 
 std::string problem_prefix(size_t i) { return "problem " + std::to_string(i) + ": "; }
+
+
 
 }  // namespace
 }  // namespace tlibttm
@@ -955,13 +968,14 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                         tcviews.push_back(v);
                         continue;
                     }
-                    // small m: the grouped TMA-fed launch where it takes the problem, else the small-m
-                    // kernels (column, row) above the single-launch size
+                    // small m: the grouped TMA-fed launch where it takes the problem; else the column and
+                    // row kernels, large problems in launches of their own, the others as work items of
+                    // the grouped small-m launch
                     if (pl.dense && v.m <= kSmallM && stream_group_eligible(v, dtype)) {
                         sgviews.push_back(v);
                         continue;
                     }
-                    if (pl.dense && v.m <= kSmallM && elems >= kPlanSingleMinElems) single = true;
+                    if (pl.dense && v.m <= kSmallM && elems >= kPlanSmallSingleMinElems) single = true;
                     if (!pl.dense || single) {
                         P->singles.push_back(Single{dtype, x.a, x.b, x.c, pl});
                     } else {
@@ -1019,23 +1033,29 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
     };
     std::stable_sort(P->singles.begin(), P->singles.end(),
                      [&](const Single& x, const Single& y) { return work(x) > work(y); });
-    int64_t first = 0;
-    for (Item& it : items) {
-        it.d.first = first;
-        first += it.d.tiles_m * it.d.tiles_n;
-        P->descs.push_back(it.d);
+    // slice-GEMM items first (one launch), then the small-m ones (the other launch); each list
+    // numbers its items from 0, largest problems first
+    for (int kind = 0; kind < 2; ++kind) {
+        int64_t first = 0;
+        for (Item& it : items) {
+            if (it.d.kind != kind) continue;
+            it.d.first = first;
+            first += it.d.tiles_m * it.d.tiles_n;
+            P->descs.push_back(it.d);
+            if (kind == 1) ++P->n_small;
+        }
+        (kind == 0 ? P->total : P->stotal) = first;
     }
-    P->total = first;
     if (!P->descs.empty()) {
         if ((e = dev_malloc(reinterpret_cast<void**>(&P->d_desc), P->descs.size() * sizeof(GroupDesc))) != cudaSuccess ||
-            (e = dev_malloc(reinterpret_cast<void**>(&P->d_queue), sizeof(unsigned long long))) != cudaSuccess)
+            (e = dev_malloc(reinterpret_cast<void**>(&P->d_queue), 2 * sizeof(unsigned long long))) != cudaSuccess)
             return fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_batched: device allocation failed.");
         if ((e = cudaMemcpy(P->d_desc, P->descs.data(), P->descs.size() * sizeof(GroupDesc), cudaMemcpyHostToDevice)) != cudaSuccess)
             return cuda_fail(e, "plan upload");
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int64_t grid = (int64_t)sms * grouped_blocks_per_sm(dtype);
-        P->grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, P->total));
+        P->grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * grouped_blocks_per_sm(dtype), P->total));
+        P->sgrid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * grouped_small_blocks_per_sm(dtype), P->stotal));
     }
     if (!tcviews.empty() && (e = tc_group_create(tcviews.data(), (int)tcviews.size(), &P->tcg)) != cudaSuccess)
         return e == cudaErrorMemoryAllocation ? fail(TLIBTTM_ERR_ALLOC, "tlibttm_plan_batched: device allocation failed.")
@@ -1138,7 +1158,10 @@ int tlibttm_plan_run_graph(tlibttm_plan* plan, void* stream)
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e;
     if (!s) {
-        if (!plan->own && (e = cudaStreamCreateWithFlags(&plan->own, cudaStreamNonBlocking)) != cudaSuccess)
+        // A graph cannot be captured on the legacy default stream; the plan's own stream is a
+        // blocking one, so that like the default stream it runs after the work already queued
+        // there (the inputs' producers) and before the work queued after it.
+        if (!plan->own && (e = cudaStreamCreateWithFlags(&plan->own, cudaStreamDefault)) != cudaSuccess)
             return cuda_fail(e, "cudaStreamCreate");
         s = plan->own;
     }
@@ -1172,6 +1195,7 @@ int tlibttm_plan_launches(const tlibttm_plan* plan)
 {
     if (!plan) return 0;
     int n = (plan->type == 0 && plan->total > 0) ? 1 : 0;
+    n += (plan->type == 0 && plan->stotal > 0) ? 1 : 0;
     n += tc_group_launches(plan->tcg) + stream_group_launches(plan->sg);
     for (const Single& sg : plan->singles) n += launches_of(sg, plan->dtype, plan->precision);
     return n;

@@ -119,6 +119,10 @@ cudaError_t launch_fill(void* p, int64_t n, int dtype, double v, cudaStream_t s)
 // (which must be zero at launch) by a persistent grid of `grid` blocks.
 cudaError_t launch_grouped(const GroupDesc* d_desc, int count, int64_t total, unsigned long long* queue, int dtype,
                            int grid, cudaStream_t s);
+// The same for small-m work items only (kind 1), with more blocks per SM.
+cudaError_t launch_grouped_small(const GroupDesc* d_desc, int count, int64_t total, unsigned long long* queue,
+                                 int dtype, int grid, cudaStream_t s);
+int grouped_small_blocks_per_sm(int dtype);
 // Row / column tile sizes of the slice-GEMM for an element type, and rows per small-m work item.
 constexpr int kGemmTileF32 = 128, kGemmTileF64 = 64, kGemvRows = 256;
 // Blocks per SM the grouped kernel is launched with.

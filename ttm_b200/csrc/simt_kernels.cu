@@ -751,8 +751,8 @@ union GroupedSmem {
     RowdotSmem<T, 16> row;
 };
 
-template <typename T, int MB>
-__device__ __forceinline__ void grouped_small(const View3& v, int flags, int64_t local, GroupedSmem<T>& sm)
+template <typename T, int MB, class SM>
+__device__ __forceinline__ void grouped_small(const View3& v, int flags, int64_t local, SM& sm)
 {
     constexpr int RV = 16 / sizeof(T);
     auto& col = reinterpret_cast<ColvecSmem<T, MB>&>(sm.col);
@@ -815,6 +815,52 @@ __global__ void __launch_bounds__(256, 2) grouped_kernel(const GroupDesc* __rest
             else if (g.m <= 8) grouped_small<T, 8>(v, g.flags, local, sm);
             else grouped_small<T, 16>(v, g.flags, local, sm);
         }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+union SmallSmem {
+    ColvecSmem<T, 16> col;
+    RowdotSmem<T, 16> row;
+};
+
+// Grouped launch of small-m problems only: the same work items as grouped_kernel's small-m ones,
+// without the slice-GEMM's registers and shared memory, so that more blocks share an SM (their
+// loads in flight are what these bandwidth-bound items need). Measured against one launch per
+// MB build (each launch leaves a tail) and against the MB = 16 build for every item (small m then
+// computes 16 columns): one launch that picks the build per item is the fastest of the three. A
+// block's items come from the queue in increasing order, so the problem search goes on from the
+// previous item's.
+template <typename T>
+__global__ void __launch_bounds__(256) grouped_small_kernel(const GroupDesc* __restrict__ desc, int count,
+                                                           int64_t total, unsigned long long* queue)
+{
+    __shared__ SmallSmem<T> sm;
+    __shared__ int64_t item_s;
+    int cur = 0;
+    for (;;) {
+        if (threadIdx.x == 0) item_s = (int64_t)atomicAdd(queue, 1ull);
+        __syncthreads();
+        const int64_t item = item_s;
+        if (item >= total) break;
+        while (cur + 1 < count && desc[cur + 1].first <= item) ++cur;
+        const GroupDesc g = desc[cur];
+        const int64_t local = item - g.first;
+        View3 v;
+        v.a = g.a;
+        v.b = g.b;
+        v.c = g.c;
+        v.outer = g.outer;
+        v.nq = g.nq;
+        v.inner = g.inner;
+        v.m = g.m;
+        v.b_cm = g.b_cm;
+        if (g.m <= 1) grouped_small<T, 1>(v, g.flags, local, sm);
+        else if (g.m <= 2) grouped_small<T, 2>(v, g.flags, local, sm);
+        else if (g.m <= 4) grouped_small<T, 4>(v, g.flags, local, sm);
+        else if (g.m <= 8) grouped_small<T, 8>(v, g.flags, local, sm);
+        else grouped_small<T, 16>(v, g.flags, local, sm);
         __syncthreads();
     }
 }
@@ -1307,6 +1353,22 @@ cudaError_t launch_grouped(const GroupDesc* d_desc, int count, int64_t total, un
 {
     if (dtype == 0) grouped_kernel<float><<<grid, 256, 0, s>>>(d_desc, count, total, queue);
     else grouped_kernel<double><<<grid, 256, 0, s>>>(d_desc, count, total, queue);
+    return cudaGetLastError();
+}
+
+int grouped_small_blocks_per_sm(int dtype)
+{
+    int n = 0;
+    cudaError_t e = dtype == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_small_kernel<float>, 256, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, grouped_small_kernel<double>, 256, 0);
+    return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+cudaError_t launch_grouped_small(const GroupDesc* d_desc, int count, int64_t total, unsigned long long* queue,
+                                 int dtype, int grid, cudaStream_t s)
+{
+    if (dtype == 0) grouped_small_kernel<float><<<grid, 256, 0, s>>>(d_desc, count, total, queue);
+    else grouped_small_kernel<double><<<grid, 256, 0, s>>>(d_desc, count, total, queue);
     return cudaGetLastError();
 }
 
