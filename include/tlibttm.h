@@ -151,7 +151,11 @@ enum tlibttm_schedule {
                                       contiguous fibres of >= 16 floats / 8 doubles on 16-byte boundaries */
     TLIBTTM_SCHED_TC_BF16X3_PAIR = 7, /* tensor-core bf16x3 on pairs of SMs with B in tensor memory, float only
                                       (128 < m <= 256, n_q <= 256; inner >= 128 or q == pia[0]) */
-    TLIBTTM_SCHED_COUNT = 8
+    TLIBTTM_SCHED_SIMT_SPLIT = 8,  /* slice-GEMM on FFMA/DFMA with its l loop split over blocks whatever the tile
+                                      count (n_q >= 2048); a fixed-order second kernel adds the parts */
+    TLIBTTM_SCHED_BVEC = 9,        /* few output rows (outer * inner <= 8), 16 < m <= 256, n_q >= 4096: B streamed
+                                      by the whole GPU, l split over blocks, fixed-order reduction */
+    TLIBTTM_SCHED_COUNT = 10
 };
 
 /* Runs one TTM with a given schedule (all operands device memory, A and C dense). */

@@ -79,7 +79,8 @@ def test_schedules_through_the_c_abi_agree(cuda):
     from ttm_b200.selector import Autotuner, valid_mask
     pr = dict(p=3, na=[64, 48, 40], q=2, pia=[1, 2, 3], m=8)
     ok = valid_mask(pr)
-    assert ok == [True, True, True, False, False, True, False]   # m = 8: neither tensor-core schedule
+    # m = 8: neither tensor-core schedule; n_q = 48: no l split, no B streaming
+    assert ok == [True, True, True, False, False, True, False, False, False]
     tuner = Autotuner(cap=1 << 20)
     t = tuner.times(pr)
     assert [x is not None for x in t] == ok and all(x > 0 for x in t if x is not None)
@@ -105,6 +106,36 @@ def test_schedules_through_the_c_abi_agree(cuda):
                                  B.data_ptr(), _lib.sz([m, na[q - 1]]), _lib.sz([1, 2]), Cc.data_ptr(), _lib.sz(nc),
                                  _lib.sz(_dense(nc, pia)), None)
     assert rc == _lib.ERR_UNSUPPORTED
+
+
+def test_split_schedules_are_tunable(cuda, oracle_c):
+    """c = B a with n = 2^16, m = 64 (order 1): the plain slice-GEMM, its l-split form (schedule 8),
+    the B-streaming kernel (9) and bf16x3 (5) are all valid; the exact ones agree with the C oracle
+    within the FP32 bound and the autotuner times each of them."""
+    import torch
+    from ttm_b200 import _lib
+    from ttm_b200.selector import Autotuner, lib, valid_mask
+    pr = dict(p=1, na=[1 << 16], q=1, pia=[1], m=64)
+    ok = valid_mask(pr)
+    assert [s for s in range(1, 10) if ok[s - 1]] == [1, 5, 8, 9]
+    t = Autotuner(cap=1 << 16, b_cap=64 << 16).times(pr)
+    assert all((t[s - 1] is not None) == ok[s - 1] for s in range(1, 10))
+    n, m = pr["na"][0], pr["m"]
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal(n).astype(np.float32)
+    b = rng.standard_normal(m * n).astype(np.float32)
+    want = np.zeros(m, dtype=np.float32)
+    oracle_c.ttm(1, a, [n], [1], [1], b, [m, n], [1, 2], want, [m], [1])
+    A, B = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+    for s in (1, 8, 9):
+        Cc = torch.full((m,), float("nan"), device=cuda)
+        _lib.check(lib().tlibttm_ttm_sched(_lib.F32, s, 1, 1, A.data_ptr(), _lib.sz([n]), _lib.sz([1]), _lib.sz([1]),
+                                           B.data_ptr(), _lib.sz([m, n]), _lib.sz([1, 2]), Cc.data_ptr(), _lib.sz([m]),
+                                           _lib.sz([1]), None))
+        torch.cuda.synchronize()
+        got = Cc.double().cpu().numpy()
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 2e-6, s
+        assert _lib.last_kernel() == ("bvec" if s == 9 else "simt_gemm"), s
 
 
 def test_small_tuning_run(cuda):

@@ -791,6 +791,8 @@ static bool sched_valid_view(int dtype, int schedule, const View3& v)
     case TLIBTTM_SCHED_TC_BF16X3: return dtype == TLIBTTM_F32 && tc_supported(v, TLIBTTM_PREC_BF16X3);
     case TLIBTTM_SCHED_COLS_TMA: return stream_supported(v, dtype);
     case TLIBTTM_SCHED_TC_BF16X3_PAIR: return dtype == TLIBTTM_F32 && tc_pair_supported(v);
+    case TLIBTTM_SCHED_SIMT_SPLIT: return v.nq >= 2048;
+    case TLIBTTM_SCHED_BVEC: return bvec_supported(v);
     default: return false;
     }
 }
@@ -834,6 +836,13 @@ int tlibttm_ttm_sched(int dtype, int schedule, unsigned q, unsigned p, const voi
     case TLIBTTM_SCHED_ROWS: return note_launch(launch_rowdot(v, dtype, s), K_ROWDOT);
     case TLIBTTM_SCHED_COLS_TMA:
         return note_launch(launch_stream(v, dtype, s), v.inner == 1 ? K_STREAM_ROWS : K_STREAM_COLS);
+    case TLIBTTM_SCHED_SIMT_SPLIT:
+    case TLIBTTM_SCHED_BVEC: {
+        int n = 1;
+        e = schedule == TLIBTTM_SCHED_BVEC ? launch_bvec(v, dtype, s, &n) : launch_simt_gemm(v, dtype, s, &n, true);
+        if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);
+        return note_launch(e, schedule == TLIBTTM_SCHED_BVEC ? K_BVEC : K_SIMT_GEMM);
+    }
     case TLIBTTM_SCHED_TC_BF16X3_PAIR: {
         int* status = nullptr;
         if ((e = tc_status_word(dev, &status)) != cudaSuccess) return cuda_fail(e, "tensor-core state");

@@ -101,7 +101,9 @@ const char* kernel_name(int id);
 // Launchers (simt_kernels.cu). Return cudaSuccess or the launch error.
 // The slice-GEMM; when its tiles cannot fill the GPU and n_q is long, the K loop is split over
 // more blocks and the parts are added by a second kernel (*launches = 2, else 1).
-cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s, int* launches = nullptr);
+// force_split: split the K loop whenever n_q >= 2048 (a schedule of its own for the tuner).
+cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s, int* launches = nullptr,
+                             bool force_split = false);
 int simt_gemm_launch_count(const View3& v, int dtype);
 // Few output rows (outer * inner <= 8), 16 < m <= 256, n_q >= 4096: a kernel that streams B with
 // the l range split over the GPU, then a fixed-order reduction (*launches = 2).

@@ -1246,16 +1246,19 @@ cudaError_t sms_of_device(int& sms)
 }
 
 // Parts of the K loop for a slice-GEMM whose tiles cannot fill the GPU (1 when none is needed).
+// `force` (a tuner's schedule): split whenever n_q >= 2048, into enough parts for two rounds of
+// blocks.
 template <typename T>
-int gemm_split_parts(const View3& v, int sms, int64_t& lper)
+int gemm_split_parts(const View3& v, int sms, int64_t& lper, bool force = false)
 {
     constexpr int RV = 16 / sizeof(T);
     constexpr int64_t BM = 32 * RV, BN = 32 * RV, BK = 8;
     const int64_t tiles = ceil_div(v.outer * v.inner, BM) * ceil_div(v.m, BN);
     const int64_t slots = (int64_t)sms * (sizeof(T) == 8 ? 3 : 2);
     lper = v.nq;
-    if (tiles * 2 > slots || v.nq < 2048) return 1;
+    if (v.nq < 2048 || (!force && tiles * 2 > slots)) return 1;
     int64_t S = std::min<int64_t>(ceil_div(slots, tiles), v.nq / 1024);
+    if (force) S = std::max<int64_t>(2, std::min<int64_t>(ceil_div(2 * slots, tiles), v.nq / 1024));
     S = std::min<int64_t>(S, 256);
     // workspace of S partial results at most 1 GiB
     const int64_t nc = v.outer * v.m * v.inner;
@@ -1266,13 +1269,13 @@ int gemm_split_parts(const View3& v, int sms, int64_t& lper)
 }
 
 template <typename T>
-cudaError_t simt_gemm_launch(const View3& v, cudaStream_t s, int* launches)
+cudaError_t simt_gemm_launch(const View3& v, cudaStream_t s, int* launches, bool force)
 {
     int sms = 0;
     cudaError_t e = sms_of_device(sms);
     if (e != cudaSuccess) return e;
     int64_t lper = 0;
-    const int S = gemm_split_parts<T>(v, sms, lper);
+    const int S = gemm_split_parts<T>(v, sms, lper, force);
     if (launches) *launches = S > 1 ? 2 : 1;
     if (S <= 1) return simt_gemm_dispatch<T>(v, s);
     const int64_t nc = v.outer * v.m * v.inner;
@@ -1290,9 +1293,10 @@ cudaError_t simt_gemm_launch(const View3& v, cudaStream_t s, int* launches)
 
 }  // namespace
 
-cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s, int* launches)
+cudaError_t launch_simt_gemm(const View3& v, int dtype, cudaStream_t s, int* launches, bool force_split)
 {
-    return dtype == 0 ? simt_gemm_launch<float>(v, s, launches) : simt_gemm_launch<double>(v, s, launches);
+    return dtype == 0 ? simt_gemm_launch<float>(v, s, launches, force_split)
+                      : simt_gemm_launch<double>(v, s, launches, force_split);
 }
 
 int simt_gemm_launch_count(const View3& v, int dtype)

@@ -34,8 +34,11 @@ try:
 except Exception:  # noqa: BLE001
     torch = None
 
-SCHEDULES = ["simt_gemm", "cols", "cols_split", "rows", "tc_bf16x3", "cols_tma", "tc_bf16x3_pair"]   # ids 1..7
-EXACT = [1, 2, 3, 4, 6]               # schedules that compute with exact FMA in the I/O type
+# ids 1..9 (include/tlibttm.h tlibttm_schedule): kernels, and for the tensor cores two tile shapes
+# (128 rows on one SM, 256 on a pair of SMs), and for the SIMT GEMM the split of the l loop
+SCHEDULES = ["simt_gemm", "cols", "cols_split", "rows", "tc_bf16x3", "cols_tma", "tc_bf16x3_pair", "simt_split",
+             "bvec"]
+EXACT = [1, 2, 3, 4, 6, 8, 9]         # schedules that compute with exact FMA in the I/O type
 NS = len(SCHEDULES)
 FEATURES = 53
 HIDDEN = 64
@@ -118,16 +121,18 @@ def valid_mask(pr, dtype_id=None):
 # ------------------------------------------------------------------------------ autotuner
 class Autotuner:
     """Times every valid schedule of a problem on scratch device buffers (inputs are random; run
-    time does not depend on values). Results are cached by problem signature."""
+    time does not depend on values). Results are cached by problem signature. `cap` bounds the
+    elements of A and of C, `b_cap` those of B; a larger problem is refused (ValueError) before
+    anything runs."""
 
-    def __init__(self, reps=3, cap=workloads.CAP, dtype_id=_lib.F32):
+    def __init__(self, reps=3, cap=workloads.CAP, dtype_id=_lib.F32, b_cap=256 * 512):
         self.reps = reps
         self.dtype_id = dtype_id
         dt = torch.float32 if dtype_id == _lib.F32 else torch.float64
         dev = torch.device("cuda", torch.cuda.current_device())
         self.A = torch.randn(cap, device=dev, dtype=dt)
         self.C = torch.empty(cap, device=dev, dtype=dt)
-        self.B = torch.randn(256 * 512, device=dev, dtype=dt)
+        self.B = torch.randn(b_cap, device=dev, dtype=dt)
         self.stream = torch.cuda.current_stream(dev)
         self.db = {}
 
@@ -149,6 +154,8 @@ class Autotuner:
         na, pia, q, m = pr["na"], pr["pia"], pr["q"], pr["m"]
         nc = list(na)
         nc[q - 1] = m
+        if math.prod(na) > self.A.numel() or math.prod(nc) > self.C.numel() or m * na[q - 1] > self.B.numel():
+            raise ValueError(f"problem {na} q={q} m={m} exceeds the tuner's scratch buffers")
         wa = _dense(na, pia)
         wc = _dense(nc, pia)
         md = [_lib.sz(na), _lib.sz(wa), _lib.sz(pia), _lib.sz([m, na[q - 1]]), _lib.sz([1, 2]), _lib.sz(nc),
@@ -179,9 +186,6 @@ class DtypeTuner:
 
     def times(self, pr):
         return self.tuners[dtype_of(pr)].times(pr)
-
-    def best(self, pr, allowed=None):
-        return self.tuners[dtype_of(pr)].best(pr, allowed)
 
     def best(self, pr, allowed=None):
         t = self.times(pr)
@@ -298,17 +302,22 @@ class Selector:
     def choose(self, pr, allowed, dtype_id=None):
         dtype_id = dtype_of(pr) if dtype_id is None else dtype_id
         ok = valid_mask(pr, dtype_id)
-        # a model trained before a schedule existed never proposes it
-        cands = [s for s in range(1, NS + 1) if ok[s - 1] and s in allowed and s <= self.model.dims[-1]]
-        if not cands:
+        valid = [s for s in range(1, NS + 1) if ok[s - 1] and s in allowed]
+        # a model trained before a schedule existed never proposes it; the autotuner times them all
+        cands = [s for s in valid if s <= self.model.dims[-1]]
+        if not valid:
             raise ValueError("no allowed schedule can run this problem")
+        if len(valid) == 1:
+            return valid[0], False
+        if len(cands) < len(valid) and self.tuner is not None and len(cands) <= 1:
+            return self.tuner.best(pr, allowed=set(valid)), True
         if len(cands) == 1:
             return cands[0], False
         X = torch.tensor([features(pr, dtype_id)], device=self.model.device)
         pred = self.model.forward(X)[0].tolist()
         ranked = sorted(cands, key=lambda s: pred[s - 1])
         if self.tuner is not None and pred[ranked[1] - 1] - pred[ranked[0] - 1] < self.margin:
-            return self.tuner.best(pr, allowed=set(cands)), True
+            return self.tuner.best(pr, allowed=set(valid)), True
         return ranked[0], False
 
 
@@ -396,6 +405,8 @@ def _heuristic_in(pr, allowed):
         w = rv if inner % rv == 0 else 1
         return 3 if math.ceil(inner * outer / (32 * w)) < 148 * 32 else 2
     ok = valid_mask(pr)
+    if 9 in allowed and ok[8]:
+        return 9
     if 7 in allowed and ok[6]:
         return 7
     if 5 in allowed and ok[4]:
