@@ -398,7 +398,7 @@ def _heuristic_in(pr, allowed):
     if pr["m"] <= 16:
         if inner == 1:
             big = math.prod(pr["na"]) * es >= 64 << 20
-            return 6 if (6 in allowed and big and nq > 16 and valid_mask(pr)[5]) else 4
+            return 6 if (6 in allowed and big and nq >= 16 and valid_mask(pr)[5]) else 4
         if 6 in allowed and math.prod(pr["na"]) * es >= 64 << 20 and valid_mask(pr)[5]:
             return 6
         rv = 16 // es
