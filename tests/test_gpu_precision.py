@@ -91,7 +91,7 @@ def test_fp8_vs_emulated_rounding(cuda, dist):
         a = draw(rng, int(np.prod(na)), dist, np.float32)
         b = draw(rng, m * na[q - 1], dist, np.float32)
         c = run_device(q, a, md, b, _lib.PREC_FP8, cuda)
-        assert _lib.last_kernel() == "tc_fp8"
+        assert _lib.last_kernel() in ("tc_fp8", "tc_fp8_pair")
         A = logical(a, na, md["wa"])
         want = fp8_ttm(q, A, b_matrix(b, md))
         C = logical(c, md["nc"], md["wc"])
@@ -135,3 +135,37 @@ def test_precision_study_small(cuda):
         assert p["bf16x3"]["kernel"].startswith("tc_bf16x3") and p["fp8"]["kernel"] == "tc_fp8"
         assert 1e-4 < p["fp8"]["rms_rel"] < 0.1
         assert p["ozaki"]["max_rel"] <= p["plain_fp32"]["max_rel"] <= p["fp8"]["max_rel"]
+
+
+# (na, pia, q, m, pib): shapes of the one-launch fp8 kernel on SM pairs (128 < m <= 256,
+# n_q <= 256, rows of >= 128 i or contiguous fibres): one and several 64-l stages, n_q not a
+# multiple of 32 or 64, partial tiles, both B layouts
+PAIR8_CASES = [([256, 40, 6], [1, 2, 3], 2, 200, [1, 2]),
+               ([200, 96, 3], [1, 2, 3], 2, 256, [2, 1]),
+               ([132, 256, 2], [1, 2, 3], 2, 130, [1, 2]),
+               ([64, 200, 50], [2, 1, 3], 2, 160, [2, 1]),
+               ([48, 36, 100], [2, 1, 3], 2, 256, [1, 2]),
+               ([128, 64, 256], [3, 1, 2], 1, 250, [2, 1])]
+
+
+@pytest.mark.parametrize("dist", ["normal", "loguniform", "integers"])
+def test_fp8_pair_kernel_vs_emulated_rounding(cuda, dist):
+    """The one-launch fp8 kernel (fibre scales found from the tile in shared memory) rounds every
+    operand exactly as the separate path does: integers come out exact, other data within the
+    FP32 accumulation of the emulated product; all-zero fibres (exponent 0) included."""
+    rng = np.random.default_rng(16)
+    for n, (na, pia, q, m, pib) in enumerate(PAIR8_CASES):
+        md = md_of(na, pia, q, m, pib)
+        a = draw(rng, int(np.prod(na)), dist, np.float32)
+        b = draw(rng, m * na[q - 1], dist, np.float32)
+        A = logical(a, na, md["wa"])
+        if n == 0:
+            np.moveaxis(A, q - 1, -1)[3, :, :] = 0.0      # a run of all-zero fibres
+        c = run_device(q, a, md, b, _lib.PREC_FP8, cuda)
+        assert _lib.last_kernel() == "tc_fp8_pair", (na, q, m)
+        want = fp8_ttm(q, A, b_matrix(b, md))
+        C = logical(c, md["nc"], md["wc"])
+        if dist == "integers":
+            assert np.array_equal(C, want), (na, q, m)
+        else:
+            assert relerr(C, want) <= 1e-5, (na, q, m, relerr(C, want))

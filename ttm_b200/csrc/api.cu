@@ -33,6 +33,7 @@ const char* kernel_name(int id)
     case K_STRIDED: return "strided";
     case K_TC_BF16X3: return "tc_bf16x3";
     case K_TC_FP8: return "tc_fp8";
+    case K_TC_FP8_PAIR: return "tc_fp8_pair";
     case K_TC_OZAKI: return "tc_ozaki";
     case K_SPLIT_B: return "split_b";
     case K_GROUPED: return "grouped";
@@ -275,6 +276,15 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s, int64_t s
             return fail(TLIBTTM_ERR_UNSUPPORTED, precision == TLIBTTM_PREC_OZAKI
                                                      ? "tlibttm: the ozaki path takes n_q <= 16384 (exact int32 sums)."
                                                      : "tlibttm: the fp8 path cannot run this problem.");
+        if (precision == TLIBTTM_PREC_FP8 && tc_pair8_supported(v)) {
+            // one launch: the fibre scales and the e4m3 operand are made from the resident tile
+            int dev = 0;
+            cudaError_t e = cudaGetDevice(&dev);
+            int* status = nullptr;
+            if (e == cudaSuccess) e = tc_status_word(dev, &status);
+            if (e == cudaSuccess) e = launch_tc_pair8(v, status, s);
+            return note_launch(e, K_TC_FP8_PAIR);
+        }
         int kid = K_NONE, n = 0;
         cudaError_t e = launch_tc8(v, precision, x.dtype, s, &kid, &n);
         if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);   // exponent and slicer kernels
@@ -612,6 +622,7 @@ int launches_of(const Single& sg, int dtype, int precision)
     int pr = precision == TLIBTTM_PREC_DEFAULT ? g_precision.load() : precision;
     if (pr == TLIBTTM_PREC_AUTO)
         pr = (dtype == TLIBTTM_F32 && tc_supported(sg.pl.v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3 : TLIBTTM_PREC_PLAIN;
+    if (pr == TLIBTTM_PREC_FP8 && tc_pair8_supported(sg.pl.v)) return 1;
     if (pr == TLIBTTM_PREC_FP8 || pr == TLIBTTM_PREC_OZAKI) return tc8_launches(sg.pl.v, pr);
     if (bvec_supported(sg.pl.v)) return 2;
     if (pr != TLIBTTM_PREC_PLAIN && tc_supported(sg.pl.v, pr)) {

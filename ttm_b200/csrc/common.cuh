@@ -93,6 +93,7 @@ enum KernelId : int {
     K_STREAM_ROWS,
     K_TC_PAIR,
     K_BVEC,
+    K_TC_FP8_PAIR,
     K_COUNT
 };
 

@@ -1,6 +1,8 @@
 // Tensor-core (tcgen05 / TMEM) paths of the B200 TTM library.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace tlibttm {
@@ -24,6 +26,18 @@ cudaError_t launch_tc_single(const View3& v, cudaStream_t s, int* kid);
 // with inner % 4 == 0. Allocates nothing; `status` is the device status word it raises.
 bool tc_pair_supported(const View3& v);
 cudaError_t launch_tc_pair(const View3& v, int* status, cudaStream_t s);
+// The pair kernels' tensor maps: A in boxes of 64 rows x 64 l (rows of i: 3-D box of 64 i x 64 l
+// x 1 k; contiguous fibres: boxes of 16 l x 64 rows, 64-byte swizzle), C in 32 x 32 blocks
+// (false when C cannot be a tensor map: the epilogue then stores directly).
+bool pair_encode_a(const View3& v, CUtensorMap* map);
+bool pair_encode_c(const View3& v, CUtensorMap* map);
+
+// fp8 on pairs of SMs (tc_pair8.cu), A read once: the shapes of tc_pair_supported. Every fibre of
+// A and row of B is scaled by 2^(8-e), max|x| = f 2^e with f in [0.5, 1), and rounded to e4m3
+// (nearest even, saturating), as the fp8 path of tc8_kernels.cu does; the scales of A's fibres
+// are found in shared memory from the resident tile, so no exponent or operand pass precedes it.
+bool tc_pair8_supported(const View3& v);
+cudaError_t launch_tc_pair8(const View3& v, int* status, cudaStream_t s);
 
 // A grouped bf16x3 launch: many float problems (each with tc_supported) whose tiles are
 // numbered one after the other and run by one persistent launch per geometry (rows of i, or

@@ -37,6 +37,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "tc_cluster.cuh"
 #include "tc_kernels.cuh"
 #include "tc_ptx.cuh"
 #include "tlibttm.h"
@@ -81,44 +82,6 @@ struct PairParams {
     unsigned long long wait_ns;
 };
 
-__device__ __forceinline__ uint32_t cluster_rank()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ uint32_t cluster_index()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
-    return r;
-}
-__device__ __forceinline__ uint32_t cluster_count()
-{
-    uint32_t r;
-    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
-    return r;
-}
-// Address of the same shared-memory variable in CTA `rank` of the cluster.
-__device__ __forceinline__ uint32_t peer_addr(uint32_t saddr, uint32_t rank)
-{
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
-    return r;
-}
-// Arrive on a barrier of another CTA of the cluster (default semantics: release at CTA scope).
-// What the arrive publishes is either shared memory the MMA reads, after fence.proxy.async, or
-// tensor memory this CTA has finished loading, after tcgen05.fence::before_thread_sync; neither
-// needs the thread's earlier global stores to be visible, which a cluster-scope release would
-// wait for.
-__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr)
-{
-    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
-}
-__device__ __forceinline__ void cluster_sync_all()
-{
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
 // D[tmem] (+)= A[tmem] * B[smem desc], both CTAs of the pair. Called by a whole converged warp
 // with warp-uniform operands; one elected lane issues the instruction.
 __device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc, uint32_t acc)
@@ -128,21 +91,6 @@ __device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint32_t tmem_a, uint6
         " @e tcgen05.mma.cta_group::2.kind::f16 [%0], [%1], %2, %3, p;\n}\n"
         ::"r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(acc)
         : "memory");
-}
-// Arrive on the barrier at this offset in every CTA of `mask` once the MMAs issued so far are
-// done (whole warp; one elected lane commits).
-__device__ __forceinline__ void commit_pair(uint64_t* bar, uint16_t mask)
-{
-    asm volatile("{\n .reg .pred e;\n elect.sync _|e, 0xffffffff;\n"
-                 " @e tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;\n}\n"
-                 ::"r"(su32(bar)), "h"(mask)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8])
-{
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
-                 ::"r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
-                 : "memory");
 }
 __device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo)
 {
@@ -573,6 +521,9 @@ cudaError_t launch_pair_geom(const CUtensorMap& amap, const CUtensorMap& cmap, c
 }
 
 }  // namespace
+
+bool pair_encode_a(const View3& v, CUtensorMap* map) { return encode_pair_map(v, v.inner == 1 ? PGEOM_K : PGEOM_MN, map); }
+bool pair_encode_c(const View3& v, CUtensorMap* map) { return encode_pair_cmap(v, v.inner == 1 ? PGEOM_K : PGEOM_MN, map); }
 
 bool tc_pair_supported(const View3& v)
 {
