@@ -358,12 +358,6 @@ __global__ void __launch_bounds__(kThreads8P, 1)
             const uint32_t fa = __float_as_uint(pow2f8(ea - 8));
             st_cluster_u32(scl0[0] + soff, fa);
             st_cluster_u32(scl0[1] + soff, fa);
-            fence_acq_rel_cluster();
-            __syncwarp();
-            if (lane == 0) {
-                mbar_arrive_remote_release_cluster(scf0[0] + (uint32_t)q * 8u);
-                mbar_arrive_remote_release_cluster(scf0[1] + (uint32_t)q * 8u);
-            }
             const int sh = 8 - ea;
             const bool fast = sh >= -126 && sh <= 127;
             const float sc = fast ? pow2f8(sh) : 1.0f;
@@ -384,6 +378,15 @@ __global__ void __launch_bounds__(kThreads8P, 1)
                     __syncwarp();
                     if (lane == 0) mbar_arrive_remote(conv0 + (uint32_t)s * 8u);
                 }
+            }
+            // the factors stored above are published now, after the conversions, so that the
+            // cluster-scope fence does not hold up the MMAs (the epilogues need them only once
+            // the tile's MMAs are done)
+            fence_acq_rel_cluster();
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive_remote_release_cluster(scf0[0] + (uint32_t)q * 8u);
+                mbar_arrive_remote_release_cluster(scf0[1] + (uint32_t)q * 8u);
             }
         }
     } else {
