@@ -372,20 +372,31 @@ def run_ours(args):
     avg_launch = statistics.mean(per_launch)
     achieved_gbs = bytes_per_ttm(S) / avg_launch / 1e9
 
+    def one_step_tflops(pr):
+        """One step (q = 1..4) of the same workload under arithmetic pr, after one untimed step."""
+        def go():
+            for q in range(1, 5):
+                _lib.ttm_raw(_lib.F32, pr, q, 4, A.data_ptr(), na, wa, pia, Bs[q - 1].data_ptr(), [S, S], [1, 2],
+                             C.data_ptr(), na, wa, sh)
+        go()
+        kname = _lib.last_kernel()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        go()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return flops_per_step(S) / (e0.elapsed_time(e1) / 1e3) / 1e12, kname
+
     # plain-FP32 comparison number (same workload, exact FFMA path), one step
     plain_tflops = None
     if prec != _lib.PREC_PLAIN:
-        for q in range(1, 5):
-            _lib.ttm_raw(_lib.F32, _lib.PREC_PLAIN, q, 4, A.data_ptr(), na, wa, pia, Bs[q - 1].data_ptr(), [S, S],
-                         [1, 2], C.data_ptr(), na, wa, sh)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for q in range(1, 5):
-            _lib.ttm_raw(_lib.F32, _lib.PREC_PLAIN, q, 4, A.data_ptr(), na, wa, pia, Bs[q - 1].data_ptr(), [S, S],
-                         [1, 2], C.data_ptr(), na, wa, sh)
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        plain_tflops = flops_per_step(S) / (e0.elapsed_time(e1) / 1e3) / 1e12
+        plain_tflops = one_step_tflops(_lib.PREC_PLAIN)[0]
+    # FP8 (e4m3 with per-fibre power-of-two scales; not FP32-accurate), one step
+    fp8 = None
+    if prec != _lib.PREC_FP8 and not args.no_extra:
+        t8, k8 = one_step_tflops(_lib.PREC_FP8)
+        fp8 = {"tflops": t8, "kernel": k8,
+               "note": "same workload at e4m3 with power-of-two fibre scales, one step; FP8 accuracy only"}
 
     extra = {}
     if not args.no_extra:
@@ -437,6 +448,7 @@ def run_ours(args):
             "rel_error_note": "24 sampled fibres per q vs float64 dot products: fro = ||c-r||/||r||, "
                               "max = max|c-r|/max|r|",
             "plain_fp32_tflops": plain_tflops,
+            "fp8": fp8,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved_gbs / hbm_peak, "traffic": traffic_per_launch(S),
                          "traffic_source": TRAFFIC_SOURCE, "peak_kind": peak_kind,

@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 8 ? 3 : 2)) simt_gemm_split
 // streams per row chunk (problems with few rows). B is staged in shared memory as [l][MB].
 // ---------------------------------------------------------------------------------------------
 constexpr int kColWarps = 8;
+constexpr int kColUnroll1 = 8;   // l steps unrolled with one scalar row per lane
 
 template <typename T, int MB>
 struct ColvecSmem {
@@ -381,7 +382,8 @@ __device__ __forceinline__ void colvec_tile(const View3& v, int64_t row0, Colvec
         }
         __syncthreads();
         if (valid) {
-#pragma unroll 4
+            // scalar rows (W = 1) take more l steps at a time, so that more loads are in flight
+#pragma unroll (W == 1 ? kColUnroll1 : 4)
             for (int l = part; l < lc; l += LS) {
                 T a[W];
                 load_vec<T, W>(a, ap + (l0 + l) * inner);
@@ -499,10 +501,22 @@ __device__ __forceinline__ void rowdot_tile(const View3& v, int64_t row0, Rowdot
                 for (int e = 0; e < RV; ++e) sm.a[warp][r][c + e] = x[e];
             }
         } else {
-            for (int r = 0; r < 32; ++r) {
-                const int64_t gr = wrow0 + r;
-                for (int c = lane; c < LC; c += 32)
-                    sm.a[warp][r][c] = (gr < rows && c < lc) ? __ldg(A + gr * nq + l0 + c) : T(0);
+            // lane c copies column c of the warp's rows: the loads of RB rows go out before their
+            // stores, so that many are in flight
+            constexpr int RB = 16;
+            const int c = lane;
+#pragma unroll 1
+            for (int rb = 0; rb < 32; rb += RB) {
+                T x[RB];
+#pragma unroll
+                for (int r = 0; r < RB; ++r) {
+                    const int64_t gr = wrow0 + rb + r;
+                    x[r] = (c < LC && c < lc && gr < rows) ? __ldg(A + gr * nq + l0 + c) : T(0);
+                }
+                if (c < LC) {
+#pragma unroll
+                    for (int r = 0; r < RB; ++r) sm.a[warp][rb + r][c] = x[r];
+                }
             }
         }
         __syncthreads();

@@ -73,15 +73,7 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
 }
 
 // x -> (hi, lo) bf16 pair, packed two at a time.
-__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo)
-{
-    __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
-    const float r0 = x0 - __low2float(h);
-    const float r1 = x1 - __high2float(h);
-    __nv_bfloat162 l = __floats2bfloat162_rn(r0, r1);
-    hi = *reinterpret_cast<uint32_t*>(&h);
-    lo = *reinterpret_cast<uint32_t*>(&l);
-}
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) { split_bf16x2(x0, x1, hi, lo); }
 
 // Byte offset of a 16-byte chunk (8 consecutive MN elements) in an MN-major SW128 bf16 tile of
 // 128 MN x 16 K laid out as [K group of 8][MN block of 64][8 K rows][64 MN].
@@ -300,10 +292,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                         continue;
                     }
                     issued[s] = (int)ph;
-                    mbar_expect_tx(&a_full[s], LA.a_bytes);
-                    // kSub boxes; a box past n_q (odd chunk count) is zero-filled by the copy
+                    // the sub-blocks within n_q (the last box's rows past n_q are zero-filled)
+                    const int nsub = min(kSub, pr.kchunks - st * kSub);
+                    mbar_expect_tx(&a_full[s], (uint32_t)nsub * LA.asub_bytes);
 #pragma unroll
                     for (int sub = 0; sub < kSub; ++sub) {
+                        if (sub >= nsub) break;
                         uint8_t* dst = a_at(s) + sub * LA.asub_bytes;
                         const int l0 = (st * kSub + sub) * kBK;
                         if (GEOM == GEOM_MN && pr.fold_kb > 1) {
@@ -398,6 +392,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint64_t db = db0 + ((uint64_t)(bs * P.bslot) >> 4);
 #pragma unroll
                     for (int sub = 0; sub < kSub; ++sub) {
+                        if (sub > 0 && st * kSub + sub >= pr.kchunks) break;   // zeros past n_q
                         const uint64_t dahi = da + (uint64_t)((sub * LA.asub_bytes) >> 4);
                         const uint64_t dalo = dahi + (uint64_t)(LA.abf_bytes >> 4);
                         const uint64_t dbhi = db + (uint64_t)((sub * 2 * b_bytes) >> 4);
@@ -431,31 +426,41 @@ __global__ void __launch_bounds__(kThreads, 1)
         const bool odd = lane & 1;
         constexpr int kIters = (kBM * kBK / 4) / (kGroupWarps * 32);
         bool ok = true;
-        int64_t n = 0;   // sequence number of the stage across this CTA's tiles
+        // The CTA's stages are numbered n = 0, 1, ... across its tiles; this group takes those with
+        // n % kConvGroups == g, which sit in ring slot n % AS with phase (n / AS) & 1. AS being a
+        // multiple of kConvGroups, the group's slot steps by kConvGroups and wraps with a phase flip.
+        int rot = 0;                 // n % kConvGroups
+        int s = g;                   // slot of the group's next stage
+        uint32_t ph = 0;
         // Every thread of a group runs every iteration of its residue and reaches the group barrier
         // the same number of times; once the CTA aborts, the waits are skipped and no work is done.
         int cur = 0;
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
             int64_t lt;
             const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
-            const int64_t mper = (pr.inner + kBM - 1) / kBM;
-            for (int st = 0; st < pr.kstages; ++st, ++n) {
-                if ((int)(n % kConvGroups) != g) continue;
-                const int s = (int)(n % AS);
-                const uint32_t ph = (uint32_t)((n / AS) & 1);
+            // tile origin for the converters' own loads of A (ldg_a): slice k / first row
+            int64_t mt = 0, tk = 0, r0 = 0;
+            if (pr.ldg_a) {
+                const int64_t mper = (pr.inner + kBM - 1) / kBM;
+                mt = lt % pr.tiles_m;
+                tk = GEOM == GEOM_MN ? mt / mper : 0;
+                r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
+            }
+            for (int st = 0; st < pr.kstages; ++st) {
+                const bool mine = rot == g;
+                if (++rot == kConvGroups) rot = 0;
+                if (!mine) continue;
                 const bool got = ok && mbar_wait(&a_full[s], ph, abort_flag, P.wait_ns);
                 const bool have = __all_sync(0xffffffffu, got);
                 if (!have) ok = false;
+                // sub-blocks past n_q are zeros that the MMA issuer skips: not converted
+                const int nsub = min(kSub, pr.kchunks - st * kSub);
 #pragma unroll 1
-                for (int sub = 0; sub < kSub; ++sub) {
+                for (int sub = 0; sub < nsub; ++sub) {
                     const int kc = st * kSub + sub;
                     uint8_t* buf = a_at(s) + sub * LA.asub_bytes;
                     float4 x[kIters];
                     uint32_t off[kIters];
-                    // tile origin for the converters' own loads of A (ldg_a): slice k / first row
-                    const int64_t mt = lt % pr.tiles_m;
-                    const int64_t tk = GEOM == GEOM_MN ? mt / mper : 0;
-                    const int64_t r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
 #pragma unroll
                     for (int it = 0; it < kIters; ++it) {
                         const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
@@ -516,6 +521,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&a_conv[s]);
                 }
+                s += kConvGroups;
+                if (s >= AS) { s -= AS; ph ^= 1; }
             }
         }
     } else {
@@ -550,7 +557,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                 r0 = mt * kBM + q4 * 32;
             }
             const int nt = pr.nt;
-            const int64_t jrem = pr.m - (int64_t)jb * nt;
+            // the record's fields the stores use, in registers: a grouped launch's records sit in
+            // global memory, where every store to C could alias them and force a reload
+            const int64_t e_inner = pr.inner, e_outer = pr.outer, e_m = pr.m;
+            float* const e_c = pr.c;
+            const bool e_tma = pr.tma_c != 0;
+            const int64_t jrem = e_m - (int64_t)jb * nt;
             const int jleft = jrem < nt ? (int)jrem : nt;
             const uint32_t tbase = tmem_base + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(ab * P.acc_stride);
             for (int cc = 0; cc < nt; cc += 32) {
@@ -558,9 +570,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tmem_ld32(tbase + (uint32_t)cc, v);
                 if (cc >= jleft) continue;
                 const int j0 = jb * nt + cc;
-                if (pr.tma_c && GEOM == GEOM_MN && k >= pr.outer) {
+                if (e_tma && GEOM == GEOM_MN && k >= e_outer) {
                     // folded last tile: this warp's slice lies past the end of C, nothing to store
-                } else if (pr.tma_c) {
+                } else if (e_tma) {
                     // Stage a 32 x 32 block in shared memory and store it with one TMA copy.
                     uint8_t* buf = stage0 + sb * kEpiBuf;
                     if (lane == 0) bulk_wait_read1();      // the copy that last read `buf` has finished reading it
@@ -585,17 +597,35 @@ __global__ void __launch_bounds__(kThreads, 1)
                         bulk_commit();
                     }
                     sb ^= 1;
-                } else {
-                    // Direct stores (C rows not 16-byte aligned for a tensor map).
+                } else if (GEOM == GEOM_MN) {
+                    // Direct stores (C rows not 16-byte aligned for a tensor map): lane = i, so each
+                    // store instruction writes 32 consecutive elements of one row j of C.
                     const int64_t r = r0 + lane;
-                    const bool rvalid = GEOM == GEOM_MN ? (r < pr.inner && k < pr.outer) : r < pr.outer;
-                    if (rvalid) {
-                        float* p = GEOM == GEOM_MN ? pr.c + (k * pr.m + j0) * pr.inner + r : pr.c + r * pr.m + j0;
-                        const int64_t cs = GEOM == GEOM_MN ? pr.inner : 1;
+                    if (r < e_inner && k < e_outer) {
+                        float* p = e_c + (k * e_m + j0) * e_inner + r;
 #pragma unroll
                         for (int c = 0; c < 32; ++c)
-                            if (cc + c < jleft) p[(int64_t)c * cs] = __uint_as_float(v[c]);
+                            if (cc + c < jleft) p[(int64_t)c * e_inner] = __uint_as_float(v[c]);
                     }
+                } else {
+                    // C rows (m elements each) not 16-byte aligned for a tensor map. A lane holds
+                    // one row of the 32 x 32 block, m elements from the next lane's row: the block
+                    // goes through shared memory ([row][col ^ row], conflict free both ways) and
+                    // out one row segment per store instruction, consecutive lanes on consecutive
+                    // elements.
+                    float* b32 = reinterpret_cast<float*>(stage0 + sb * kEpiBuf);
+                    if (lane == 0) bulk_wait_read0();      // no TMA store is still reading it
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) b32[lane * 32 + (c ^ lane)] = __uint_as_float(v[c]);
+                    __syncwarp();
+                    const int cw = jleft - cc < 32 ? jleft - cc : 32;
+                    const int64_t rl = e_outer - r0;
+                    const int nrow = rl < 32 ? (int)rl : 32;
+                    float* cb = e_c + r0 * e_m + j0 + lane;
+                    if (lane < cw)
+                        for (int row = 0; row < nrow; ++row) cb[(int64_t)row * e_m] = b32[row * 32 + (lane ^ row)];
+                    __syncwarp();
                 }
             }
             tc_fence_before();

@@ -92,13 +92,7 @@ __device__ __forceinline__ void mma_pair(uint32_t tmem_d, uint32_t tmem_a, uint6
         ::"r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(acc)
         : "memory");
 }
-__device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo)
-{
-    __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
-    __nv_bfloat162 l = __floats2bfloat162_rn(x0 - __low2float(h), x1 - __high2float(h));
-    hi = *reinterpret_cast<uint32_t*>(&h);
-    lo = *reinterpret_cast<uint32_t*>(&l);
-}
+__device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uint32_t& lo) { split_bf16x2(x0, x1, hi, lo); }
 // Byte offset of the 16-byte chunk of 8 consecutive rows (`rchunk`) at l (0..15) in an MN-major
 // 128-byte-swizzled bf16 part of 64 rows x 16 l: [l / 8][l % 8][64 rows, chunk ^ (l % 8)].
 __device__ __forceinline__ uint32_t mn64_off(uint32_t l, uint32_t rchunk)
@@ -277,12 +271,16 @@ __global__ void __launch_bounds__(kThreadsP, 1)
         const uint32_t conv0 = peer_addr(su32(&a_conv[0]), 0);      // the even CTA's a_conv[0]
         constexpr int kIt = (int)(kStageBytes / 16) / (kGroupWarpsP * 32);   // float4 per thread per stage
         bool ok = true;
-        int64_t n = 0;   // stage sequence number across this cluster's tiles
+        // Stages are numbered n = 0, 1, ... across this cluster's tiles; this group takes those with
+        // n % kConvGroupsP == g, in ring slot n % AS with phase (n / AS) & 1. AS being a multiple
+        // of kConvGroupsP, the group's slot steps by kConvGroupsP and wraps with a phase flip.
+        int rot = 0, s = g;
+        uint32_t ph = 0;
         for (int64_t t = cid; t < tiles; t += ncl) {
-            for (int st = 0; st < kst; ++st, ++n) {
-                if ((int)(n % kConvGroupsP) != g) continue;
-                const int s = (int)(n % AS);
-                const uint32_t ph = (uint32_t)((n / AS) & 1);
+            for (int st = 0; st < kst; ++st) {
+                const bool mine = rot == g;
+                if (++rot == kConvGroupsP) rot = 0;
+                if (!mine) continue;
                 const bool got = ok && mbar_wait(&a_full[s], ph, abort_flag, P.wait_ns);
                 const bool have = __all_sync(0xffffffffu, got);
                 if (!have) ok = false;
@@ -325,6 +323,8 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                     __syncwarp();
                     if (lane == 0) mbar_arrive_remote(conv0 + (uint32_t)s * 8u);
                 }
+                s += kConvGroupsP;
+                if (s >= AS) { s -= AS; ph ^= 1; }
             }
         }
     } else {
