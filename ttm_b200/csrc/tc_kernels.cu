@@ -438,15 +438,29 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
             int64_t lt;
             const TcProb& pr = tile_problem<GROUP>(one, P, t, cur, lt);
+            // the record's fields in registers (stores through generic pointers could alias a
+            // grouped launch's records in global memory and force reloads); those of the
+            // converters' own loads only where they load A
+            const int kst = pr.kstages, kch = pr.kchunks;
+            const bool ldg = pr.ldg_a != 0;
+            const float* ga = nullptr;
+            int64_t gnq = 0, ginner = 0, gouter = 0;
+            int fkb = 1, fsh = 0;
             // tile origin for the converters' own loads of A (ldg_a): slice k / first row
             int64_t mt = 0, tk = 0, r0 = 0;
-            if (pr.ldg_a) {
-                const int64_t mper = (pr.inner + kBM - 1) / kBM;
+            if (ldg) {
+                ga = pr.a;
+                gnq = pr.nq;
+                ginner = pr.inner;
+                gouter = pr.outer;
+                fkb = pr.fold_kb;
+                fsh = pr.fold_ib_shift;
+                const int64_t mper = (ginner + kBM - 1) / kBM;
                 mt = lt % pr.tiles_m;
                 tk = GEOM == GEOM_MN ? mt / mper : 0;
                 r0 = GEOM == GEOM_MN ? (mt - tk * mper) * kBM : mt * kBM;
             }
-            for (int st = 0; st < pr.kstages; ++st) {
+            for (int st = 0; st < kst; ++st) {
                 const bool mine = rot == g;
                 if (++rot == kConvGroups) rot = 0;
                 if (!mine) continue;
@@ -454,7 +468,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const bool have = __all_sync(0xffffffffu, got);
                 if (!have) ok = false;
                 // sub-blocks past n_q are zeros that the MMA issuer skips: not converted
-                const int nsub = min(kSub, pr.kchunks - st * kSub);
+                const int nsub = min(kSub, kch - st * kSub);
 #pragma unroll 1
                 for (int sub = 0; sub < nsub; ++sub) {
                     const int kc = st * kSub + sub;
@@ -466,33 +480,33 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const int v = gt + kGroupWarps * 32 * it;   // float4 index within the 8 KB tile
                         if (GEOM == GEOM_MN) {
                             const int l = v >> 5, w = v & 31;               // [16 l][128 i], 512-byte rows
-                            if (have && pr.ldg_a) {
+                            if (have && ldg) {
                                 // elements (l, i .. i+3) of slice tk (of slice tk * KB + row / IB when
                                 // folded), zero outside A
                                 const int64_t gl = (int64_t)kc * kBK + l;
-                                const int64_t sk = pr.fold_kb > 1 ? mt * pr.fold_kb + ((w * 4) >> pr.fold_ib_shift) : tk;
-                                const int64_t i = pr.fold_kb > 1 ? ((w * 4) & ((1 << pr.fold_ib_shift) - 1)) : r0 + w * 4;
-                                const float* src = pr.a + (sk * pr.nq + gl) * pr.inner + i;
-                                const bool lv = gl < pr.nq && sk < pr.outer;
-                                x[it].x = (lv && i < pr.inner) ? __ldg(src) : 0.0f;
-                                x[it].y = (lv && i + 1 < pr.inner) ? __ldg(src + 1) : 0.0f;
-                                x[it].z = (lv && i + 2 < pr.inner) ? __ldg(src + 2) : 0.0f;
-                                x[it].w = (lv && i + 3 < pr.inner) ? __ldg(src + 3) : 0.0f;
+                                const int64_t sk = fkb > 1 ? mt * fkb + ((w * 4) >> fsh) : tk;
+                                const int64_t i = fkb > 1 ? ((w * 4) & ((1 << fsh) - 1)) : r0 + w * 4;
+                                const float* src = ga + (sk * gnq + gl) * ginner + i;
+                                const bool lv = gl < gnq && sk < gouter;
+                                x[it].x = (lv && i < ginner) ? __ldg(src) : 0.0f;
+                                x[it].y = (lv && i + 1 < ginner) ? __ldg(src + 1) : 0.0f;
+                                x[it].z = (lv && i + 2 < ginner) ? __ldg(src + 2) : 0.0f;
+                                x[it].w = (lv && i + 3 < ginner) ? __ldg(src + 3) : 0.0f;
                             } else if (have) {
                                 x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
                             }
                             off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
                         } else {
                             const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
-                            if (have && pr.ldg_a) {
+                            if (have && ldg) {
                                 // elements (row, l .. l+3) of the contiguous fibre row, zero outside A
                                 const int64_t row = r0 + k, gl = (int64_t)kc * kBK + lc * 4;
-                                const float* src = pr.a + row * pr.nq + gl;
-                                const bool rv = row < pr.outer;
-                                x[it].x = (rv && gl < pr.nq) ? __ldg(src) : 0.0f;
-                                x[it].y = (rv && gl + 1 < pr.nq) ? __ldg(src + 1) : 0.0f;
-                                x[it].z = (rv && gl + 2 < pr.nq) ? __ldg(src + 2) : 0.0f;
-                                x[it].w = (rv && gl + 3 < pr.nq) ? __ldg(src + 3) : 0.0f;
+                                const float* src = ga + row * gnq + gl;
+                                const bool rv = row < gouter;
+                                x[it].x = (rv && gl < gnq) ? __ldg(src) : 0.0f;
+                                x[it].y = (rv && gl + 1 < gnq) ? __ldg(src + 1) : 0.0f;
+                                x[it].z = (rv && gl + 2 < gnq) ? __ldg(src + 2) : 0.0f;
+                                x[it].w = (rv && gl + 3 < gnq) ? __ldg(src + 3) : 0.0f;
                             } else if (have) {
                                 x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
                             }
@@ -883,7 +897,11 @@ __global__ void __maxnreg__(stream_nreg(CPS))
         for (int64_t u = blockIdx.x; u < L.total; u += gridDim.x) {
             int64_t lu;
             const StreamProb& pq = unit_problem<GROUP>(one, L, u, cur, lu);
-            const StreamParams& Q = pq.P;
+            // a grouped launch's record by value: its fields in global memory could otherwise be
+            // aliased by the stores to C and to B's staging area and reloaded after each (a single
+            // launch's record is a constant kernel parameter)
+            const StreamParams Qv = pq.P;
+            const StreamParams& Q = GROUP ? Qv : pq.P;
             const int S = Q.S;
             const int IB = 1 << Q.ib_shift;
             const int kk = pos >> (Q.ib_shift + Q.h_shift);
