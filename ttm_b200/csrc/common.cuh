@@ -136,6 +136,36 @@ constexpr int64_t kSmallM = 16;
 
 __host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Division of 32-bit unsigned n by a divisor d fixed at set-up, by multiplication (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", 1994): with l = ceil(log2 d)
+// and mul = floor(2^32 (2^l - d) / d) + 1, n / d = (mulhi(n, mul) + n) >> l for every n < 2^32,
+// the sum taken in 64 bits. Kernels use it where a runtime divisor would otherwise cost an
+// integer division sequence per tile and thread.
+struct FastDiv {
+    uint32_t d, mul, shift;
+};
+
+inline FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f;
+    f.d = d < 1 ? 1 : d;
+    uint32_t l = 0;
+    while ((uint64_t(1) << l) < f.d) ++l;
+    f.shift = l;
+    f.mul = (uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << l) - f.d)) / f.d + 1);
+    return f;
+}
+
+__host__ __device__ inline uint32_t fast_div(uint32_t n, const FastDiv& f)
+{
+#ifdef __CUDA_ARCH__
+    const uint32_t hi = __umulhi(n, f.mul);
+#else
+    const uint32_t hi = (uint32_t)(((uint64_t)n * f.mul) >> 32);
+#endif
+    return (uint32_t)(((uint64_t)hi + n) >> f.shift);
+}
+
 // Every device allocation of the library goes through these two wrappers (cudaMalloc and the
 // stream-ordered cudaMallocAsync), so that a test can make the n-th one fail (tlibttm_inject).
 cudaError_t dev_malloc(void** p, size_t bytes);

@@ -744,6 +744,7 @@ struct StreamParams {
     int ib_shift;           // log2(IB)
     int h_shift;            // log2(H); H > 1 uses the 4D map
     int kb;                 // KB = P / (IB * H)
+    FastDiv fd_s, fd_mper;  // division by S and by mper (unit -> tile -> slice block)
 };
 
 // One problem of a stream launch: its tensor map and parameters. A single launch passes it as a
@@ -857,9 +858,9 @@ __global__ void __maxnreg__(stream_nreg(CPS))
                 const StreamParams& Q = pq.P;
                 const int S = Q.S;
                 const int IB = 1 << Q.ib_shift;
-                const int64_t t = lu / S;
+                const int64_t t = S == 1 ? lu : (int64_t)fast_div((uint32_t)lu, Q.fd_s);
                 const int r = (int)(lu - t * S);
-                const int64_t kb = t / Q.mper, ib = t - kb * Q.mper;
+                const int64_t kb = fast_div((uint32_t)t, Q.fd_mper), ib = t - kb * Q.mper;
                 const int kc0 = r * Q.kper, kc1 = min(kc0 + Q.kper, Q.kchunks);
                 for (int kc = kc0; kc < kc1; ++kc) {
                     if (!mbar_wait(&empty[s], ph ^ 1, abort_flag)) { ok = false; break; }
@@ -908,9 +909,9 @@ __global__ void __maxnreg__(stream_nreg(CPS))
             const int hh = (pos >> Q.ib_shift) & ((1 << Q.h_shift) - 1), ii = pos & (IB - 1);
             const T* Bg = static_cast<const T*>(Q.b);
             T* C = static_cast<T*>(Q.c);
-            const int64_t t = lu / S;
+            const int64_t t = S == 1 ? lu : (int64_t)fast_div((uint32_t)lu, Q.fd_s);
             const int r = (int)(lu - t * S);
-            const int64_t kb = t / Q.mper, ib = t - kb * Q.mper;
+            const int64_t kb = fast_div((uint32_t)t, Q.fd_mper), ib = t - kb * Q.mper;
             const int kc0 = r * Q.kper, kc1 = min(kc0 + Q.kper, Q.kchunks);
             if (r != staged || cur != staged_p) {
                 // stage rows [kc0 * lb, kc1 * lb) of B: bs[l][j] = B(j, l), zero outside B. The
@@ -1775,6 +1776,9 @@ void fill_stream_params(const View3& v, const StreamShape& sh, StreamParams& P)
     P.ib_shift = sh.ib_shift;
     P.h_shift = sh.h_shift;
     P.kb = sh.kb;
+    // unit and tile indices fit in 32 bits: a tile holds 256 or more positions
+    P.fd_s = make_fastdiv((uint32_t)sh.S);
+    P.fd_mper = make_fastdiv((uint32_t)sh.mper);
 }
 
 bool stream_supported(const View3& v, int dtype)
