@@ -444,6 +444,149 @@ __global__ void __launch_bounds__(256) colvec_kernel(View3 v)
     colvec_tile<T, MB, W, LS>(v, (int64_t)blockIdx.x * (kColWarps / LS) * 32 * W, sm);
 }
 
+// colvec_async: the column kernel for rows without 16-byte alignment (one row per lane). Each
+// thread streams its own row's elements A[k][l][i] into a ring of shared memory with 4- or 8-byte
+// asynchronous copies (cp.async, any 4-byte alignment), kColAsyncStages - 1 stages of kColAsyncL
+// l ahead of the one it multiplies, so that many loads are in flight without holding them in
+// registers. A thread reads back only what it copied itself: the ring needs no block barrier,
+// only the thread's own wait on its copy groups. B is staged per chunk of LB l as in colvec.
+constexpr int kColAsyncStages = 3;
+constexpr bool kColAsync = true;   // rows without 16-byte alignment take colvec_async
+
+template <typename T, int MB>
+struct ColvecAsyncSmem {
+    static constexpr int MBP = MB < 4 ? 4 : MB;
+    static constexpr int LC = sizeof(T) == 8 ? 4 : 8;                      // l per stage
+    static constexpr int LB = sizeof(T) == 8 ? 128 : 256;                  // l of B per chunk
+    __align__(16) T a[kColAsyncStages][LC][256];
+    __align__(16) T bs[LB][MBP];
+    __align__(16) T red[kColWarps][32];
+};
+
+__device__ __forceinline__ void cp_async_elem(void* smem_dst, const void* src, int bytes, int src_bytes)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T, int MB, int LS>
+__device__ __forceinline__ void colvec_async_tile(const View3& v, int64_t row0, ColvecAsyncSmem<T, MB>& sm)
+{
+    using SM = ColvecAsyncSmem<T, MB>;
+    constexpr int LB = SM::LB, LC = SM::LC, MBP = SM::MBP, ST = kColAsyncStages;
+    const T* __restrict__ A = static_cast<const T*>(v.a);
+    const T* __restrict__ B = static_cast<const T*>(v.b);
+    T* __restrict__ Cp = static_cast<T*>(v.c);
+    const int64_t inner = v.inner, nq = v.nq, m = v.m;
+    const int64_t M = v.outer * inner;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int chunk = warp / LS, part = warp % LS;
+    const int64_t row = row0 + (int64_t)chunk * 32 + lane;
+    const bool valid = row < M;
+    const int64_t k = valid ? row / inner : 0;
+    const int64_t i = valid ? row - k * inner : 0;
+    const T* ap = A + k * inner * nq + i;
+
+    T acc[MB];
+#pragma unroll
+    for (int j = 0; j < MB; ++j) acc[j] = T(0);
+
+    for (int64_t l0 = 0; l0 < nq; l0 += LB) {
+        const int lc = (int)((nq - l0) < LB ? (nq - l0) : LB);
+        __syncthreads();
+        for (int e = tid; e < lc * MBP; e += blockDim.x) {
+            const int l = e / MBP, j = e % MBP;
+            const int64_t gl = l0 + l;
+            sm.bs[l][j] = (j < m) ? (v.b_cm ? B[j + gl * m] : B[j * nq + gl]) : T(0);
+        }
+        __syncthreads();
+        // this thread's l in the chunk: part, part + LS, ...; n of them, in stages of LC
+        const int n = lc > part ? (lc - part + LS - 1) / LS : 0;
+        const int nst = (n + LC - 1) / LC;
+        const T* base = ap + l0 * inner;
+        auto issue = [&](int st) {
+            T* dst = &sm.a[st % ST][0][tid];
+#pragma unroll
+            for (int c = 0; c < LC; ++c) {
+                const int idx = st * LC + c;
+                const bool ok = valid && idx < n;
+                cp_async_elem(dst + c * 256, ok ? base + (int64_t)(part + idx * LS) * inner : A, (int)sizeof(T),
+                              ok ? (int)sizeof(T) : 0);
+            }
+        };
+        // one commit group per stage (empty ones too), so that wait_group counts stages
+#pragma unroll
+        for (int st = 0; st < ST - 1; ++st) {
+            if (st < nst) issue(st);
+            cp_async_commit();
+        }
+        for (int st = 0; st < nst; ++st) {
+            // refill the slot the previous stage used, then wait for this stage's copies
+            if (st + ST - 1 < nst) issue(st + ST - 1);
+            cp_async_commit();
+            cp_async_wait<ST - 1>();
+#pragma unroll
+            for (int c = 0; c < LC; ++c) {
+                const int idx = st * LC + c;
+                if (idx >= n) break;
+                const T a = sm.a[st % ST][c][tid];
+                const int l = part + idx * LS;
+                T bj[MBP];
+                if constexpr (MBP * sizeof(T) % 16 == 0) {
+#pragma unroll
+                    for (int q = 0; q < MBP * (int)sizeof(T) / 16; ++q) {
+                        typename V16<T>::type t = *reinterpret_cast<const typename V16<T>::type*>(&sm.bs[l][q * (16 / sizeof(T))]);
+#pragma unroll
+                        for (int e = 0; e < (int)(16 / sizeof(T)); ++e) bj[q * (16 / sizeof(T)) + e] = reinterpret_cast<const T*>(&t)[e];
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < MBP; ++j) bj[j] = sm.bs[l][j];
+                }
+#pragma unroll
+                for (int j = 0; j < MB; ++j) acc[j] = fma_t(a, bj[j], acc[j]);
+            }
+        }
+        cp_async_wait<0>();   // no copy into the ring is pending when the next chunk restarts it
+    }
+    T* cp = Cp + k * inner * m + i;
+    if constexpr (LS == 1) {
+        if (valid) {
+#pragma unroll
+            for (int j = 0; j < MB; ++j)
+                if (j < m) cp[j * inner] = acc[j];
+        }
+    } else {
+        // Reduce the LS warps' partial sums, one output column at a time.
+#pragma unroll
+        for (int j = 0; j < MB; ++j) {
+            if (j >= m) break;
+            __syncthreads();
+            sm.red[warp][lane] = acc[j];
+            __syncthreads();
+            if (part == 0 && valid) {
+                T t = T(0);
+#pragma unroll
+                for (int q = 0; q < LS; ++q) t += sm.red[chunk * LS + q][lane];
+                cp[j * inner] = t;
+            }
+        }
+    }
+}
+
+template <typename T, int MB, int LS>
+__global__ void __launch_bounds__(256) colvec_async_kernel(View3 v)
+{
+    __shared__ ColvecAsyncSmem<T, MB> sm;
+    colvec_async_tile<T, MB, LS>(v, (int64_t)blockIdx.x * (kColWarps / LS) * 32, sm);
+}
+
 // ---------------------------------------------------------------------------------------------
 // rowdot: small m (<= MB), contiguous fibres (inner == 1): C[k][j] = sum_l A[k][l] B(j,l).
 // Each warp owns 32 rows; the block walks l in chunks of LC = 128/sizeof(T): every warp copies
@@ -765,7 +908,8 @@ union GroupedSmem {
     RowdotSmem<T, 16> row;
 };
 
-template <typename T, int MB, class SM>
+// ASYNC: unaligned column items take colvec_async (its ring must be part of SM).
+template <typename T, int MB, bool ASYNC, class SM>
 __device__ __forceinline__ void grouped_small(const View3& v, int flags, int64_t local, SM& sm)
 {
     constexpr int RV = 16 / sizeof(T);
@@ -776,6 +920,7 @@ __device__ __forceinline__ void grouped_small(const View3& v, int flags, int64_t
         else rowdot_tile<T, MB, false>(v, local * 256, row);
     } else {
         if (flags & 2) colvec_tile<T, MB, RV, 1>(v, local * kColWarps * 32 * RV, col);
+        else if constexpr (ASYNC) colvec_async_tile<T, MB, 1>(v, local * kColWarps * 32, reinterpret_cast<ColvecAsyncSmem<T, MB>&>(sm.cola));
         else colvec_tile<T, MB, 1, 1>(v, local * kColWarps * 32, col);
     }
 }
@@ -823,11 +968,11 @@ __global__ void __launch_bounds__(256, 2) grouped_kernel(const GroupDesc* __rest
                 else     { if (g.b_cm) gemm_tile<T, false, false, true>(v, m0, n0, sm.gemm); else gemm_tile<T, false, false, false>(v, m0, n0, sm.gemm); }
             }
         } else {
-            if (g.m <= 1) grouped_small<T, 1>(v, g.flags, local, sm);
-            else if (g.m <= 2) grouped_small<T, 2>(v, g.flags, local, sm);
-            else if (g.m <= 4) grouped_small<T, 4>(v, g.flags, local, sm);
-            else if (g.m <= 8) grouped_small<T, 8>(v, g.flags, local, sm);
-            else grouped_small<T, 16>(v, g.flags, local, sm);
+            if (g.m <= 1) grouped_small<T, 1, false>(v, g.flags, local, sm);
+            else if (g.m <= 2) grouped_small<T, 2, false>(v, g.flags, local, sm);
+            else if (g.m <= 4) grouped_small<T, 4, false>(v, g.flags, local, sm);
+            else if (g.m <= 8) grouped_small<T, 8, false>(v, g.flags, local, sm);
+            else grouped_small<T, 16, false>(v, g.flags, local, sm);
         }
         __syncthreads();
     }
@@ -836,6 +981,7 @@ __global__ void __launch_bounds__(256, 2) grouped_kernel(const GroupDesc* __rest
 template <typename T>
 union SmallSmem {
     ColvecSmem<T, 16> col;
+    ColvecAsyncSmem<T, 16> cola;
     RowdotSmem<T, 16> row;
 };
 
@@ -870,11 +1016,11 @@ __global__ void __launch_bounds__(256) grouped_small_kernel(const GroupDesc* __r
         v.inner = g.inner;
         v.m = g.m;
         v.b_cm = g.b_cm;
-        if (g.m <= 1) grouped_small<T, 1>(v, g.flags, local, sm);
-        else if (g.m <= 2) grouped_small<T, 2>(v, g.flags, local, sm);
-        else if (g.m <= 4) grouped_small<T, 4>(v, g.flags, local, sm);
-        else if (g.m <= 8) grouped_small<T, 8>(v, g.flags, local, sm);
-        else grouped_small<T, 16>(v, g.flags, local, sm);
+        if (g.m <= 1) grouped_small<T, 1, kColAsync>(v, g.flags, local, sm);
+        else if (g.m <= 2) grouped_small<T, 2, kColAsync>(v, g.flags, local, sm);
+        else if (g.m <= 4) grouped_small<T, 4, kColAsync>(v, g.flags, local, sm);
+        else if (g.m <= 8) grouped_small<T, 8, kColAsync>(v, g.flags, local, sm);
+        else grouped_small<T, 16, kColAsync>(v, g.flags, local, sm);
         __syncthreads();
     }
 }
@@ -914,11 +1060,17 @@ cudaError_t colvec_dispatch_ls(const View3& v, cudaStream_t s)
 {
     const int64_t M = v.outer * v.inner;
     dim3 grid((unsigned)ceil_div(M, (kColWarps / LS) * 32 * W)), block(256);
-    if (v.m <= 1) colvec_kernel<T, 1, W, LS><<<grid, block, 0, s>>>(v);
-    else if (v.m <= 2) colvec_kernel<T, 2, W, LS><<<grid, block, 0, s>>>(v);
-    else if (v.m <= 4) colvec_kernel<T, 4, W, LS><<<grid, block, 0, s>>>(v);
-    else if (v.m <= 8) colvec_kernel<T, 8, W, LS><<<grid, block, 0, s>>>(v);
-    else colvec_kernel<T, 16, W, LS><<<grid, block, 0, s>>>(v);
+#define TLIBTTM_COLVEC(MBv)                                                                \
+    do {                                                                                   \
+        if (W == 1 && kColAsync) colvec_async_kernel<T, MBv, LS><<<grid, block, 0, s>>>(v); \
+        else colvec_kernel<T, MBv, W, LS><<<grid, block, 0, s>>>(v);                       \
+    } while (0)
+    if (v.m <= 1) TLIBTTM_COLVEC(1);
+    else if (v.m <= 2) TLIBTTM_COLVEC(2);
+    else if (v.m <= 4) TLIBTTM_COLVEC(4);
+    else if (v.m <= 8) TLIBTTM_COLVEC(8);
+    else TLIBTTM_COLVEC(16);
+#undef TLIBTTM_COLVEC
     return cudaGetLastError();
 }
 
