@@ -450,14 +450,14 @@ __global__ void __launch_bounds__(256) colvec_kernel(View3 v)
 // l ahead of the one it multiplies, so that many loads are in flight without holding them in
 // registers. A thread reads back only what it copied itself: the ring needs no block barrier,
 // only the thread's own wait on its copy groups. B is staged per chunk of LB l as in colvec.
-constexpr int kColAsyncStages = 3;
+constexpr int kColAsyncStages = 4;
 constexpr bool kColAsync = true;   // rows without 16-byte alignment take colvec_async
 
 template <typename T, int MB>
 struct ColvecAsyncSmem {
     static constexpr int MBP = MB < 4 ? 4 : MB;
     static constexpr int LC = sizeof(T) == 8 ? 4 : 8;                      // l per stage
-    static constexpr int LB = sizeof(T) == 8 ? 128 : 256;                  // l of B per chunk
+    static constexpr int LB = sizeof(T) == 8 ? 64 : 128;                   // l of B per chunk
     __align__(16) T a[kColAsyncStages][LC][256];
     __align__(16) T bs[LB][MBP];
     __align__(16) T red[kColWarps][32];
