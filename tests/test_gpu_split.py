@@ -4,6 +4,8 @@
   order-1 product c = B a (reference include/tlib/detail/mtm.h:171-177, 212-218): B is streamed
   by the whole GPU, each block's partial sums go to a workspace and a second kernel adds them in
   a fixed block order.
+  The same kernels take small m (m <= 16) with few rows, where the column and row kernels would
+  run one or two blocks.
 * the SIMT slice-GEMM with its K loop split over blocks (few row x column tiles, long l range),
   partial tiles added in a fixed order.
 
@@ -74,6 +76,33 @@ def test_bvec_against_oracle(cuda, oracle_c, case, dtype):
     if dtype == np.float32:
         _, _, auto, _, kern = _run(cuda, na, pia, q, m, b_cm, dtype, precision=_lib.PREC_AUTO, a=a, b=b)
         assert kern == "bvec" and np.array_equal(got, auto)
+
+
+SMALL_M_FEW_ROWS = [
+    # (na, pia, q, m, b_cm)           m <= 16, outer * inner <= 8 rows, n_q >= 4096
+    ([1 << 16, 2], [2, 1], 1, 8, True),    # two rows 2 apart (inner 2): not 16-byte aligned
+    ([5001, 3], [1, 2], 1, 5, False),      # three contiguous fibres of odd length, row-major B
+    ([4097], [1], 1, 1, True),             # order 1, m = 1: one dot product
+    ([7, 8192], [1, 2], 2, 16, True),      # seven rows (inner 7)
+    ([1 << 15, 8], [1, 2], 1, 3, True),    # eight aligned fibres, A below the TMA kernel's size
+]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("case", SMALL_M_FEW_ROWS)
+def test_small_m_few_rows_take_the_l_split(cuda, oracle_c, case, dtype):
+    """Small m with a handful of output rows and a long l range: the column and row kernels would
+    run one or two blocks over the whole range, so the l range is split over the GPU (the bvec
+    kernels and their fixed-order reduction), exact and deterministic."""
+    na, pia, q, m, b_cm = case
+    n0 = _lib.launch_count()
+    a, b, got, md, kern = _run(cuda, na, pia, q, m, b_cm, dtype)
+    assert kern == "bvec", kern
+    assert _lib.launch_count() - n0 == 2
+    err = _check(oracle_c, q, a, b, got, md)
+    assert err <= TOL[dtype], (case, err)
+    _, _, again, _, _ = _run(cuda, na, pia, q, m, b_cm, dtype, a=a, b=b)
+    assert np.array_equal(got, again)
 
 
 SPLIT_CASES = [

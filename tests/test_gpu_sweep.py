@@ -11,5 +11,5 @@ def test_sweep_subset(cuda):
     res = sweep(dtypes=("f32",), ms=(1, 64), n_layouts=1, reps=1, log=lambda s: None)
     assert len(res["cases"]) == 2 * sum(len(n) for n in extent_sets())
     for c in res["cases"]:
-        assert c["gbs"] > 0 and c["kernel"] in ("rowdot", "colvec", "stream_cols", "stream_rows", "simt_gemm")
+        assert c["gbs"] > 0 and c["kernel"] in ("rowdot", "colvec", "stream_cols", "stream_rows", "simt_gemm", "bvec")
     assert set(res["summary"]) == {"f32_m1", "f32_m64"}

@@ -253,6 +253,14 @@ int run_device(const Args& x, Plan& pl, int precision, cudaStream_t s, int64_t s
         // TMA-fed row mode measured 0.87-0.88 of HBM against 0.65-0.72 at m = 8).
         const int64_t a_bytes = v.outer * v.nq * v.inner * (x.dtype == TLIBTTM_F32 ? 4 : 8);
         const bool tma = a_bytes >= stream_min_bytes && stream_supported(v, x.dtype);
+        // Few rows (outer * inner <= 8) and a long l range the TMA kernel does not take: the
+        // column and row kernels would run a block or two; the l range goes over the GPU instead.
+        if (!tma && bvec_small_supported(v)) {
+            int n = 1;
+            cudaError_t e = launch_bvec(v, x.dtype, s, &n);
+            if (e == cudaSuccess && n > 1) g_launches += (unsigned long long)(n - 1);
+            return note_launch(e, K_BVEC);
+        }
         if (v.inner == 1) {
             if (tma && v.nq >= 16) return note_launch(launch_stream(v, x.dtype, s), K_STREAM_ROWS);
             return note_launch(launch_rowdot(v, x.dtype, s), K_ROWDOT);
@@ -618,7 +626,12 @@ int run_single(Single& sg, int precision, cudaStream_t s)
 int launches_of(const Single& sg, int dtype, int precision)
 {
     if (!sg.pl.dense) return 1;
-    if (sg.pl.v.m <= kSmallM) return 1;
+    if (sg.pl.v.m <= kSmallM) {
+        const View3& v = sg.pl.v;
+        const int64_t a_bytes = v.outer * v.nq * v.inner * (dtype == TLIBTTM_F32 ? 4 : 8);
+        const bool tma = a_bytes >= kPlanStreamMinBytes && stream_supported(v, dtype);
+        return (!tma && bvec_small_supported(v)) ? 2 : 1;
+    }
     int pr = precision == TLIBTTM_PREC_DEFAULT ? g_precision.load() : precision;
     if (pr == TLIBTTM_PREC_AUTO)
         pr = (dtype == TLIBTTM_F32 && tc_supported(sg.pl.v, TLIBTTM_PREC_BF16X3)) ? TLIBTTM_PREC_BF16X3 : TLIBTTM_PREC_PLAIN;
@@ -997,6 +1010,8 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                         continue;
                     }
                     if (pl.dense && v.m <= kSmallM && elems >= kPlanSmallSingleMinElems) single = true;
+                    // few rows and a long l range: the l-split launch (a work item would be one block)
+                    if (pl.dense && bvec_small_supported(v)) single = true;
                     if (!pl.dense || single) {
                         P->singles.push_back(Single{dtype, x.a, x.b, x.c, pl});
                     } else {

@@ -109,6 +109,8 @@ int simt_gemm_launch_count(const View3& v, int dtype);
 // Few output rows (outer * inner <= 8), 16 < m <= 256, n_q >= 4096: a kernel that streams B with
 // the l range split over the GPU, then a fixed-order reduction (*launches = 2).
 bool bvec_supported(const View3& v);
+// The same split for small m (m <= kSmallM): few rows and n_q >= 4096.
+bool bvec_small_supported(const View3& v);
 cudaError_t launch_bvec(const View3& v, int dtype, cudaStream_t s, int* launches = nullptr);
 cudaError_t launch_colvec(const View3& v, int dtype, cudaStream_t s);
 // colvec with an explicit l split over warps (1 or 8).

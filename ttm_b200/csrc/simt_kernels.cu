@@ -1479,6 +1479,11 @@ bool bvec_supported(const View3& v)
     return v.m > kSmallM && v.m <= kBvecMaxM && v.outer * v.inner <= kBvecMaxR && v.nq >= 4096;
 }
 
+bool bvec_small_supported(const View3& v)
+{
+    return v.m >= 1 && v.m <= kSmallM && v.outer * v.inner <= kBvecMaxR && v.nq >= 4096;
+}
+
 cudaError_t launch_bvec(const View3& v, int dtype, cudaStream_t s, int* launches)
 {
     int sms = 0;
