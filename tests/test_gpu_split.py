@@ -85,15 +85,21 @@ SMALL_M_FEW_ROWS = [
     ([4097], [1], 1, 1, True),             # order 1, m = 1: one dot product
     ([7, 8192], [1, 2], 2, 16, True),      # seven rows (inner 7)
     ([1 << 15, 8], [1, 2], 1, 3, True),    # eight aligned fibres, A below the TMA kernel's size
+    # more than eight rows: row tiles of eight along the grid
+    ([63, 16411], [1, 2], 2, 8, True),     # 63 strided rows (a partial last tile)
+    ([2049, 1023], [1, 2], 1, 16, False),  # 1023 contiguous fibres, row-major B
+    ([5, 7, 17000], [1, 2, 3], 3, 1, True),  # 35 rows over two modes, m = 1
+    ([9, 1100, 11], [2, 1, 3], 2, 4, False),  # q = pi_1 with outer 99 rows, row-major B
 ]
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("case", SMALL_M_FEW_ROWS)
 def test_small_m_few_rows_take_the_l_split(cuda, oracle_c, case, dtype):
-    """Small m with a handful of output rows and a long l range: the column and row kernels would
-    run one or two blocks over the whole range, so the l range is split over the GPU (the bvec
-    kernels and their fixed-order reduction), exact and deterministic."""
+    """Small m with few output rows and a long l range: the column and row kernels would run one
+    or a few blocks over the whole range, so the l range is split over the GPU (the bvec kernels,
+    row tiles of eight beyond eight rows, and their fixed-order reduction), exact and
+    deterministic."""
     na, pia, q, m, b_cm = case
     n0 = _lib.launch_count()
     a, b, got, md, kern = _run(cuda, na, pia, q, m, b_cm, dtype)

@@ -1201,11 +1201,26 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(const T* __restrict__
 // W = 16 / sizeof(T) when the vector accesses are aligned (VEC), else 1.
 // ---------------------------------------------------------------------------------------------
 constexpr int kBvecMaxR = 8, kBvecMaxM = 256, kBvecTile = 1024;
+constexpr int64_t kBvecSmallMaxRows = 65536;   // small m: row tiles of 8 up to this many rows
 
-template <typename T, int R>
-__device__ __forceinline__ T bvec_a(const T* __restrict__ A, const View3& v, int r, int64_t l)
+// Offsets in A of (row r0 + r, l = 0) for the R rows of a row tile (r = k inner + i); A's element
+// (row, l) is then at offset + l inner.
+template <int R>
+__device__ __forceinline__ void bvec_rows(const View3& v, int64_t r0, int Rv, int64_t (&off)[R])
 {
-    const int64_t k = r / v.inner, i = r - k * v.inner;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int64_t row = r0 + (r < Rv ? r : 0);
+        const int64_t k = row / v.inner, i = row - k * v.inner;
+        off[r] = k * v.nq * v.inner + i;
+    }
+}
+
+// A's element (row, l), row = k inner + i
+template <typename T>
+__device__ __forceinline__ T bvec_a(const T* __restrict__ A, const View3& v, int64_t row, int64_t l)
+{
+    const int64_t k = row / v.inner, i = row - k * v.inner;
     return __ldg(A + (k * v.nq + l) * v.inner + i);
 }
 
@@ -1221,7 +1236,11 @@ __global__ void __launch_bounds__(256) bvec_cm_kernel(View3 v, int64_t lper, T* 
     const int JV = (int)((m + W - 1) / W), LS = 256 / JV;
     const int tid = threadIdx.x, jv = tid % JV, ls = tid / JV;
     const int64_t l0 = (int64_t)blockIdx.x * lper, l1 = l0 + lper < v.nq ? l0 + lper : v.nq;
-    const int Rv = (int)(v.outer * v.inner);
+    // rows r0 .. r0 + R - 1 of this block's row tile (blockIdx.y), Rv of them in A
+    const int64_t r0 = (int64_t)blockIdx.y * R, rrem = v.outer * v.inner - r0;
+    const int Rv = (int)(rrem < R ? rrem : R);
+    int64_t aoff[R];
+    bvec_rows<R>(v, r0, Rv, aoff);
     T acc[W][R];
 #pragma unroll
     for (int w = 0; w < W; ++w)
@@ -1232,7 +1251,7 @@ __global__ void __launch_bounds__(256) bvec_cm_kernel(View3 v, int64_t lper, T* 
         for (int64_t l = l0 + ls; l < l1; l += LS) {
             T a[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[r] = r < Rv ? bvec_a<T, R>(A, v, r, l) : T(0);
+            for (int r = 0; r < R; ++r) a[r] = r < Rv ? __ldg(A + aoff[r] + l * v.inner) : T(0);
             T b[W];
             const T* bp = B + l * m + (int64_t)jv * W;
             if constexpr (VEC) {
@@ -1258,7 +1277,8 @@ __global__ void __launch_bounds__(256) bvec_cm_kernel(View3 v, int64_t lper, T* 
         }
     }
     __syncthreads();
-    T* wb = ws + (size_t)blockIdx.x * (size_t)(R * m);
+    // ws[g][row][j] over all row tiles: this block's rows start at r0
+    T* wb = ws + ((size_t)blockIdx.x * gridDim.y * R + (size_t)r0) * (size_t)m;
     for (int e = tid; e < R * m; e += 256) {
         T sum = red[e];
         for (int q = 1; q < LS; ++q) sum += red[(size_t)q * R * m + e];
@@ -1276,7 +1296,8 @@ __global__ void __launch_bounds__(256) bvec_rm_kernel(View3 v, int64_t lper, T* 
     const int64_t m = v.m, nq = v.nq;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t l0 = (int64_t)blockIdx.x * lper, l1 = l0 + lper < nq ? l0 + lper : nq;
-    const int Rv = (int)(v.outer * v.inner);
+    const int64_t r0 = (int64_t)blockIdx.y * R, rrem = v.outer * v.inner - r0;
+    const int Rv = (int)(rrem < R ? rrem : R);
     for (int e = tid; e < R * kBvecMaxM; e += 256) part[e / kBvecMaxM][e % kBvecMaxM] = T(0);
     __syncthreads();
     for (int64_t t0 = l0; t0 < l1; t0 += kBvecTile) {
@@ -1303,12 +1324,12 @@ __global__ void __launch_bounds__(256) bvec_rm_kernel(View3 v, int64_t lper, T* 
 #pragma unroll
                         for (int w = 0; w < W; ++w)
 #pragma unroll
-                            for (int r = 0; r < R; ++r) a[w][r] = r < Rv ? bvec_a<T, R>(A, v, r, l + w) : T(0);
+                            for (int r = 0; r < R; ++r) a[w][r] = r < Rv ? bvec_a<T>(A, v, r0 + r, l + w) : T(0);
                     }
                 } else {
                     b[0] = __ldg(bj + l);
 #pragma unroll
-                    for (int r = 0; r < R; ++r) a[0][r] = r < Rv ? bvec_a<T, R>(A, v, r, l) : T(0);
+                    for (int r = 0; r < R; ++r) a[0][r] = r < Rv ? bvec_a<T>(A, v, r0 + r, l) : T(0);
                 }
 #pragma unroll
                 for (int w = 0; w < W; ++w)
@@ -1327,7 +1348,7 @@ __global__ void __launch_bounds__(256) bvec_rm_kernel(View3 v, int64_t lper, T* 
         }
     }
     __syncthreads();
-    T* wb = ws + (size_t)blockIdx.x * (size_t)(R * m);
+    T* wb = ws + ((size_t)blockIdx.x * gridDim.y * R + (size_t)r0) * (size_t)m;
     for (int e = tid; e < R * m; e += 256) wb[e] = part[e / m][e % m];
 }
 
@@ -1348,7 +1369,7 @@ __global__ void __launch_bounds__(256) bvec_reduce_kernel(const T* __restrict__ 
 }
 
 template <typename T, int R>
-cudaError_t bvec_launch_r(const View3& v, int G, int64_t lper, bool vec, T* ws, cudaStream_t s)
+cudaError_t bvec_launch_r(const View3& v, dim3 G, int64_t lper, bool vec, T* ws, cudaStream_t s)
 {
     if (v.b_cm) {
         constexpr int WV = 16 / (int)sizeof(T);
@@ -1370,26 +1391,31 @@ cudaError_t bvec_dispatch(const View3& v, int sms, cudaStream_t s, int* launches
     constexpr int WV = 16 / (int)sizeof(T);
     const int64_t R = v.outer * v.inner;
     const int Rt = R <= 1 ? 1 : R <= 2 ? 2 : R <= 4 ? 4 : 8;
+    // more than 8 rows (small m only): row tiles of 8 along the grid's y dimension
+    const int64_t ty = ceil_div(R, Rt);
     // 16-byte accesses: B's j vectors (column-major) or l vectors (row-major; for one row also A's)
     bool vec = aligned16(v.b) && (v.b_cm ? v.m % WV == 0 : v.nq % WV == 0);
     if (!v.b_cm && Rt == 1) vec = vec && v.inner == 1 && aligned16(v.a);
     // contiguous l ranges of at least 4096 l, eight blocks per SM at most; starts on vector boundaries
-    const int G = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(v.nq, 4096), (int64_t)sms * 8));
+    // (with row tiles: about eight blocks per SM over all tiles, l ranges of at least 1024 l)
+    const int G = ty == 1 ? (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(v.nq, 4096), (int64_t)sms * 8))
+                          : (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(v.nq, 1024), ceil_div((int64_t)sms * 8, ty)));
     const int64_t lper = ceil_div(ceil_div(v.nq, G), WV) * WV;
     const int Gr = (int)ceil_div(v.nq, lper);
     T* ws = nullptr;
-    cudaError_t e = dev_malloc_async(reinterpret_cast<void**>(&ws), (size_t)Gr * Rt * v.m * sizeof(T), s);
+    cudaError_t e = dev_malloc_async(reinterpret_cast<void**>(&ws), (size_t)Gr * ty * Rt * v.m * sizeof(T), s);
     if (e != cudaSuccess) return e;
+    const dim3 grid((unsigned)Gr, (unsigned)ty);
     switch (Rt) {
-    case 1: e = bvec_launch_r<T, 1>(v, Gr, lper, vec, ws, s); break;
-    case 2: e = bvec_launch_r<T, 2>(v, Gr, lper, vec, ws, s); break;
-    case 4: e = bvec_launch_r<T, 4>(v, Gr, lper, vec, ws, s); break;
-    default: e = bvec_launch_r<T, 8>(v, Gr, lper, vec, ws, s); break;
+    case 1: e = bvec_launch_r<T, 1>(v, grid, lper, vec, ws, s); break;
+    case 2: e = bvec_launch_r<T, 2>(v, grid, lper, vec, ws, s); break;
+    case 4: e = bvec_launch_r<T, 4>(v, grid, lper, vec, ws, s); break;
+    default: e = bvec_launch_r<T, 8>(v, grid, lper, vec, ws, s); break;
     }
     if (e == cudaSuccess) {
-        const int64_t n = (int64_t)Rt * v.m;
+        const int64_t n = ty * Rt * v.m;
         bvec_reduce_kernel<T><<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), 1024)), 256, 0, s>>>(
-            ws, Gr, v, Rt);
+            ws, Gr, v, (int)(ty * Rt));
         e = cudaGetLastError();
     }
     cudaFreeAsync(ws, s);
@@ -1481,7 +1507,13 @@ bool bvec_supported(const View3& v)
 
 bool bvec_small_supported(const View3& v)
 {
-    return v.m >= 1 && v.m <= kSmallM && v.outer * v.inner <= kBvecMaxR && v.nq >= 4096;
+    const int64_t R = v.outer * v.inner;
+    if (v.m < 1 || v.m > kSmallM) return false;
+    if (R <= kBvecMaxR) return v.nq >= 4096;
+    // row tiles: rows too few for the column and row kernels to fill the GPU, l long enough to
+    // split (measured at m = 8, 16-4095 rows: against the row kernel from n_q = 1024 on, against
+    // the column kernel's l-split form only for long l ranges)
+    return R <= kBvecSmallMaxRows && v.nq >= (v.inner == 1 ? 1024 : 16384);
 }
 
 cudaError_t launch_bvec(const View3& v, int dtype, cudaStream_t s, int* launches)
