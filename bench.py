@@ -241,6 +241,13 @@ def run_extra_workloads(dev, stream):
                           "note": "one batched plan (small problems in one grouped persistent launch, the others "
                                   "as single launches over 4 worker streams), CUDA graph replay"}
     plan.close()
+    # the same set with TLIBTTM_PLAN_FEW_LAUNCHES (every small-m problem in the grouped launch)
+    plan = BatchPlan(entries, precision="auto", few_launches=True)
+    t = _time_graph(plan, stream)
+    out["batched_512_few_launches"] = {"tflops": fl / t / 1e12, "gbs": by / t / 1e9, "ms": 1e3 * t,
+                                       "launches_per_run": plan.launches,
+                                       "note": "same problems and buffers, plan option TLIBTTM_PLAN_FEW_LAUNCHES"}
+    plan.close()
     del entries
     S, r = 192, 32
     A = torch.randn(S ** 4, device=dev, generator=gen)

@@ -207,17 +207,27 @@ typedef struct tlibttm_problem {
 } tlibttm_problem;
 
 /*
- * Batched plan: `count` independent TTMs of one dtype. Small dense problems run
- * in ONE persistent grouped launch whose blocks pull work items (slice-GEMM tiles
- * or row blocks of small-m problems, largest problems first) from a device work
- * queue. Problems of at least 2^18 elements of A (tensor-core ones under
- * precision bf16x3/auto, small-m ones always) and problems with non-dense strides
- * get their own launch of the kernel the planner picks; these run largest first
- * on worker streams the plan owns, forked from `stream` and joined back into it.
- * Errors name the offending problem ("problem 7: ...").
+ * Batched plan: `count` independent TTMs of one dtype, in grouped persistent launches:
+ * every float problem bf16x3 takes (precision bf16x3, or auto with m > 16) in one
+ * tensor-core launch per geometry; small-m problems the TMA-fed kernel takes in one
+ * launch per kernel build; the other small-m problems as row-block work items of one
+ * launch, except those of at least 2^22 elements of A and those with few rows and a long
+ * l range, which get their own launch; the other slice-GEMM problems as tiles of one
+ * launch. Problems with non-dense strides get their own launch. Single launches run
+ * largest first on worker streams the plan owns, forked from `stream` and joined back
+ * into it. Errors name the offending problem ("problem 7: ...").
+ * (Reference counterpart: none; the reference runs one TTM per call, ttm.h:100-138.)
  */
 int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_problem* problems,
                          tlibttm_plan** plan);
+
+/* tlibttm_plan_batched with options. TLIBTTM_PLAN_FEW_LAUNCHES: small-m problems of any
+ * size become work items of the grouped small-m launch (fewer launches per run, for callers
+ * that launch eagerly rather than replay a graph; measured 4-5 % slower on the 512-problem
+ * benchmark set under graph replay). */
+#define TLIBTTM_PLAN_FEW_LAUNCHES 1u
+int tlibttm_plan_batched_ex(int dtype, int precision, size_t count, const tlibttm_problem* problems,
+                            unsigned flags, tlibttm_plan** plan);
 
 /*
  * Chain plan (Tucker projection, ttmpy.ttms): C = A x_{modes[0]} B_0 x_{modes[1]} B_1 ... in

@@ -246,3 +246,46 @@ def test_graph_replay_without_a_stream_waits_for_queued_work(cuda):
         for pr, c in zip(probs, c0):
             assert torch.allclose(pr["C"], c, rtol=1e-5, atol=1e-5), rnd
     plan.close()
+
+
+FEW_LAUNCH_CASES = [
+    # (na, pia, q, m): small-m problems of at least 2^22 elements, rows not 16-byte aligned (by
+    # default each takes a launch of its own), and two slice-GEMM ones
+    ([129, 130, 251], [1, 2, 3], 3, 5),
+    ([129, 130, 251], [1, 2, 3], 2, 9),
+    ([131, 257, 125], [1, 2, 3], 1, 7),
+    ([125, 131, 257], [2, 1, 3], 3, 16),
+    ([64, 48, 40], [1, 2, 3], 2, 40),
+    ([48, 64, 40], [3, 1, 2], 1, 24),
+]
+
+
+@pytest.mark.parametrize("precision", ["plain", "auto"])
+def test_batched_plan_few_launches(cuda, precision):
+    """TLIBTTM_PLAN_FEW_LAUNCHES puts the large small-m problems into the grouped small-m launch:
+    fewer launches, the same results within the exact paths' bound."""
+    import torch
+    from ttm_b200.plans import BatchPlan
+    g = torch.Generator(device=cuda).manual_seed(5)
+    runs = {}
+    for few in (False, True):
+        probs = []
+        for na, pia, q, m in FEW_LAUNCH_CASES:
+            nq = na[q - 1]
+            A = torch.randn(int(np.prod(na)), device=cuda, generator=g)
+            B = torch.randn(m, nq, device=cuda, generator=g)
+            Cc = torch.full((int(np.prod(na)) // nq * m,), float("nan"), device=cuda)
+            probs.append(dict(q=q, A=A, B=B, C=Cc, na=na, pia=pia, m=m))
+        plan = BatchPlan(probs, precision=precision, few_launches=few)
+        plan.run_graph()
+        torch.cuda.synchronize()
+        worst = 0.0
+        for pr in probs:
+            want = _ref(pr["A"].double().cpu().numpy(), pr["na"], pr["pia"], pr["q"], pr["B"].double().cpu().numpy())
+            got = pr["C"].double().cpu().numpy()
+            worst = max(worst, np.linalg.norm(got - want) / np.linalg.norm(want))
+        assert worst <= (1e-5 if precision == "auto" else 2e-6), (few, worst)
+        runs[few] = plan.launches
+        plan.close()
+    assert runs[True] < runs[False], runs
+    assert runs[True] <= 8, runs

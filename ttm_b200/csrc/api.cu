@@ -945,7 +945,16 @@ int tlibttm_ttm_f32_bf16x3_noalloc(unsigned q, unsigned p, const float* a, const
 int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_problem* problems,
                          tlibttm_plan** plan)
 {
+    return tlibttm_plan_batched_ex(dtype, precision, count, problems, 0u, plan);
+}
+
+int tlibttm_plan_batched_ex(int dtype, int precision, size_t count, const tlibttm_problem* problems,
+                            unsigned flags, tlibttm_plan** plan)
+{
     if (!plan) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_batched: plan pointer is null.");
+    if (flags & ~TLIBTTM_PLAN_FEW_LAUNCHES) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_batched_ex: unknown flags.");
+    // small-m problems of at least this many elements of A get launches of their own
+    const int64_t small_single_min = (flags & TLIBTTM_PLAN_FEW_LAUNCHES) ? INT64_MAX : kPlanSmallSingleMinElems;
     *plan = nullptr;
     if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
     if (precision < TLIBTTM_PREC_DEFAULT || precision > TLIBTTM_PREC_AUTO)
@@ -1009,7 +1018,7 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                         sgviews.push_back(v);
                         continue;
                     }
-                    if (pl.dense && v.m <= kSmallM && elems >= kPlanSmallSingleMinElems) single = true;
+                    if (pl.dense && v.m <= kSmallM && elems >= small_single_min) single = true;
                     // few rows and a long l range: the l-split launch (a work item would be one block)
                     if (pl.dense && bvec_small_supported(v)) single = true;
                     if (!pl.dense || single) {
@@ -1028,16 +1037,14 @@ int tlibttm_plan_batched(int dtype, int precision, size_t count, const tlibttm_p
                         const int64_t rv = 16 / (int64_t)es;
                         if (v.m <= kSmallM) {
                             d.kind = 1;
-                            const bool al = (reinterpret_cast<uintptr_t>(v.a) % 16 == 0) && (reinterpret_cast<uintptr_t>(v.c) % 16 == 0);
-                            // work items: 256 rows (contiguous fibres) or 32*W rows (strided fibres,
-                            // W = 16-byte width when aligned) -- the tile sizes of rowdot / colvec
+                            // work items: 256 rows (contiguous fibres) or 256 rows of one per lane
+                            // (strided fibres) -- the tile sizes of rowdot / colvec_async
                             if (v.inner == 1) {
                                 d.flags = 1 | ((reinterpret_cast<uintptr_t>(v.a) % 16 == 0 && v.nq % rv == 0) ? 2 : 0);
                                 d.tiles_m = ceil_div(M, kGemvRows);
-                            } else if (al && v.inner % rv == 0) {
-                                d.flags = 2;
-                                d.tiles_m = ceil_div(M, 8 * 32 * rv);
                             } else {
+                                // column items: one row per lane (the asynchronous-copy tile takes
+                                // any alignment; a 16-byte build would cost the launch registers)
                                 d.flags = 0;
                                 d.tiles_m = ceil_div(M, 8 * 32);
                             }

@@ -919,7 +919,7 @@ __device__ __forceinline__ void grouped_small(const View3& v, int flags, int64_t
         if (flags & 2) rowdot_tile<T, MB, true>(v, local * 256, row);
         else rowdot_tile<T, MB, false>(v, local * 256, row);
     } else {
-        if (flags & 2) colvec_tile<T, MB, RV, 1>(v, local * kColWarps * 32 * RV, col);
+        if (!ASYNC && (flags & 2)) colvec_tile<T, MB, RV, 1>(v, local * kColWarps * 32 * RV, col);
         else if constexpr (ASYNC) colvec_async_tile<T, MB, 1>(v, local * kColWarps * 32, reinterpret_cast<ColvecAsyncSmem<T, MB>&>(sm.cola));
         else colvec_tile<T, MB, 1, 1>(v, local * kColWarps * 32, col);
     }
@@ -993,7 +993,7 @@ union SmallSmem {
 // block's items come from the queue in increasing order, so the problem search goes on from the
 // previous item's.
 template <typename T>
-__global__ void __launch_bounds__(256) grouped_small_kernel(const GroupDesc* __restrict__ desc, int count,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) grouped_small_kernel(const GroupDesc* __restrict__ desc, int count,
                                                            int64_t total, unsigned long long* queue)
 {
     __shared__ SmallSmem<T> sm;

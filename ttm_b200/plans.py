@@ -32,6 +32,9 @@ def _declare(L):
         return
     L.tlibttm_plan_batched.restype = C.c_int
     L.tlibttm_plan_batched.argtypes = [C.c_int, C.c_int, C.c_size_t, C.POINTER(_Problem), C.POINTER(C.c_void_p)]
+    L.tlibttm_plan_batched_ex.restype = C.c_int
+    L.tlibttm_plan_batched_ex.argtypes = [C.c_int, C.c_int, C.c_size_t, C.POINTER(_Problem), C.c_uint,
+                                          C.POINTER(C.c_void_p)]
     L.tlibttm_plan_chain.restype = C.c_int
     L.tlibttm_plan_chain.argtypes = [C.c_int, C.c_int, C.c_uint, C.c_void_p, C.POINTER(C.c_size_t),
                                      C.POINTER(C.c_size_t), C.c_uint, C.POINTER(C.c_uint),
@@ -94,9 +97,13 @@ class BatchPlan(_Plan):
 
     A_i and C_i are dense torch CUDA tensors in memory order with layout ``pia`` (one-based,
     fastest mode first; their shapes are the mode extents in mode order); B_i has shape (m, n_q)
-    and is read row-major (or column-major when ``b_cm``)."""
+    and is read row-major (or column-major when ``b_cm``). ``few_launches``: small-m problems of
+    any size share the grouped small-m launch (fewer launches per run; for eager launching rather
+    than graph replay)."""
 
-    def __init__(self, problems, precision="default"):
+    FEW_LAUNCHES = 1
+
+    def __init__(self, problems, precision="default", few_launches=False):
         super().__init__()
         L = _lib.lib()
         _declare(L)
@@ -115,9 +122,10 @@ class BatchPlan(_Plan):
                               Cc.data_ptr(), meta[5], meta[6])
             dt = _dtype(A)
         self._keep.append(arr)
-        _lib.check(L.tlibttm_plan_batched(dt if dt is not None else _lib.F32, _lib.PRECISIONS.get(precision, precision)
-                                          if isinstance(precision, str) else int(precision), len(problems), arr,
-                                          C.byref(self._h)))
+        _lib.check(L.tlibttm_plan_batched_ex(dt if dt is not None else _lib.F32,
+                                             _lib.PRECISIONS.get(precision, precision)
+                                             if isinstance(precision, str) else int(precision), len(problems), arr,
+                                             self.FEW_LAUNCHES if few_launches else 0, C.byref(self._h)))
 
 
 class ChainPlan(_Plan):
