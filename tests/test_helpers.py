@@ -161,3 +161,42 @@ def test_printer_matches_reference_text(tmp_path):
     got = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
     want = open(os.path.join(ROOT, "tests", "golden", "printer_ref.txt")).read()
     assert got == want
+
+
+FASTDIV_PROBE = r"""
+#include "common.cuh"
+#include <cstdio>
+int main() {
+    using namespace tlibttm;
+    uint64_t s = 88172645463325252ull;
+    auto rnd = [&]() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return s; };
+    long bad = 0;
+    for (uint32_t t = 0; t < 100000; ++t) {
+        uint32_t d = t < 50000 ? t + 1 : (uint32_t)(rnd() >> (rnd() % 33 + 31));
+        if (!d) d = 1;
+        const FastDiv f = make_fastdiv(d);
+        const uint32_t ns[6] = {0u, 1u, d - 1, d, 0xffffffffu, (uint32_t)rnd()};
+        for (uint32_t n : ns) bad += fast_div(n, f) != n / d;
+        for (int k = 0; k < 8; ++k) { const uint32_t n = (uint32_t)rnd(); bad += fast_div(n, f) != n / d; }
+    }
+    std::printf("%ld\n", bad);
+    return bad != 0;
+}
+"""
+
+
+def test_fast_division_by_invariant_divisors(tmp_path):
+    """The multiplicative divisors the stream kernel uses for its unit -> tile -> slice indices
+    (common.cuh, host build of the same code) equal integer division: divisors 1..50000 and
+    random ones up to 2^32 - 1, numerators 0, 1, d - 1, d, 2^32 - 1 and random."""
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("g++ not available")
+    cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    src = tmp_path / "fastdiv.cpp"
+    src.write_text(FASTDIV_PROBE)
+    exe = tmp_path / "fastdiv"
+    subprocess.run([gxx, "-std=c++17", "-O2", "-I", os.path.join(ROOT, "ttm_b200", "csrc"), "-I",
+                    os.path.join(cuda_home, "include"), str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "0", r.stdout
