@@ -171,7 +171,6 @@ __host__ inline bool choose_stages(int nt, int& as, int& bs, size_t& smem)
     return true;
 }
 
-__device__ __forceinline__ uint4 pack4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) { return make_uint4(a, b, c, d); }
 
 // Named barrier of one converter group (ids 1..kConvGroups; id 0 is __syncthreads).
 __device__ __forceinline__ void conv_barrier(int g)
@@ -520,13 +519,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                             uint32_t h0, l0, h1, l1;
                             split2(x[it].x, x[it].y, h0, l0);
                             split2(x[it].z, x[it].w, h1, l1);
-                            // Lane pairs hold 8 consecutive elements: the even lane assembles the hi
-                            // chunk, the odd lane the lo chunk.
-                            const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
-                            const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
-                            const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
-                            if (!odd) *reinterpret_cast<uint4*>(buf + off[it]) = pack4(h0, h1, got0, got1);
-                            else *reinterpret_cast<uint4*>(buf + LA.abf_bytes + off[it]) = pack4(got0, got1, l0, l1);
+                            // Lane pairs hold 8 consecutive elements, one 16-byte chunk of each part:
+                            // each lane writes its half of the hi and of the lo chunk.
+                            const uint32_t half = odd ? 8u : 0u;
+                            *reinterpret_cast<uint2*>(buf + off[it] + half) = make_uint2(h0, h1);
+                            *reinterpret_cast<uint2*>(buf + LA.abf_bytes + off[it] + half) = make_uint2(l0, l1);
                         }
                     }
                 }

@@ -311,13 +311,11 @@ __global__ void __launch_bounds__(kThreadsP, 1)
                         uint32_t h0, l0, h1, l1;
                         split_pair(x[it].x, x[it].y, h0, l0);
                         split_pair(x[it].z, x[it].w, h1, l1);
-                        // lane pairs hold 8 consecutive elements: the even lane writes the hi
-                        // chunk, the odd lane the lo chunk
-                        const uint32_t give0 = odd ? h0 : l0, give1 = odd ? h1 : l1;
-                        const uint32_t got0 = __shfl_xor_sync(0xffffffffu, give0, 1);
-                        const uint32_t got1 = __shfl_xor_sync(0xffffffffu, give1, 1);
-                        if (!odd) *reinterpret_cast<uint4*>(buf + off[it]) = make_uint4(h0, h1, got0, got1);
-                        else *reinterpret_cast<uint4*>(buf + kPartBytes + off[it]) = make_uint4(got0, got1, l0, l1);
+                        // lane pairs hold 8 consecutive elements, one 16-byte chunk of each part:
+                        // each lane writes its half of the hi and of the lo chunk
+                        const uint32_t half = odd ? 8u : 0u;
+                        *reinterpret_cast<uint2*>(buf + off[it] + half) = make_uint2(h0, h1);
+                        *reinterpret_cast<uint2*>(buf + kPartBytes + off[it] + half) = make_uint2(l0, l1);
                     }
                     fence_proxy_async();
                     __syncwarp();
