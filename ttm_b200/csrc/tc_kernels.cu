@@ -424,6 +424,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int gt = threadIdx.x - 96 - g * kGroupWarps * 32;   // 0 .. kGroupWarps*32-1
         const bool odd = lane & 1;
         constexpr int kIters = (kBM * kBK / 4) / (kGroupWarps * 32);
+        // this thread's float4 positions in a sub-block: where it reads the FP32 tile and where
+        // its 16-byte chunks of the bf16 parts go (the same for every sub-block)
+        uint32_t rdo[kIters], wro[kIters];
+#pragma unroll
+        for (int it = 0; it < kIters; ++it) {
+            const int v = gt + kGroupWarps * 32 * it;
+            if (GEOM == GEOM_MN) {
+                const int l = v >> 5, w = v & 31;
+                rdo[it] = (uint32_t)(l * 512 + w * 16);
+                wro[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
+            } else {
+                const int k = v >> 2, lc = v & 3;
+                rdo[it] = (uint32_t)(k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                wro[it] = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
+            }
+        }
         bool ok = true;
         // The CTA's stages are numbered n = 0, 1, ... across its tiles; this group takes those with
         // n % kConvGroups == g, which sit in ring slot n % AS with phase (n / AS) & 1. AS being a
@@ -492,9 +508,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 x[it].z = (lv && i + 2 < ginner) ? __ldg(src + 2) : 0.0f;
                                 x[it].w = (lv && i + 3 < ginner) ? __ldg(src + 3) : 0.0f;
                             } else if (have) {
-                                x[it] = *reinterpret_cast<const float4*>(buf + l * 512 + w * 16);
+                                x[it] = *reinterpret_cast<const float4*>(buf + rdo[it]);
                             }
-                            off[it] = mnmaj_sw128_off((uint32_t)l, (uint32_t)(w >> 1));
+                            off[it] = wro[it];
                         } else {
                             const int k = v >> 2, lc = v & 3;               // [128 k][16 l], TMA 64B swizzle
                             if (have && ldg) {
@@ -507,9 +523,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 x[it].z = (rv && gl + 2 < gnq) ? __ldg(src + 2) : 0.0f;
                                 x[it].w = (rv && gl + 3 < gnq) ? __ldg(src + 3) : 0.0f;
                             } else if (have) {
-                                x[it] = *reinterpret_cast<const float4*>(buf + k * 64 + ((lc ^ ((k >> 1) & 3)) << 4));
+                                x[it] = *reinterpret_cast<const float4*>(buf + rdo[it]);
                             }
-                            off[it] = kmaj_sw32_off((uint32_t)k, (uint32_t)(lc >> 1));
+                            off[it] = wro[it];
                         }
                     }
                     conv_barrier(g);   // the whole FP32 tile is in registers before it is overwritten
