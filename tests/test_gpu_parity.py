@@ -417,3 +417,37 @@ def test_pipelined_host_staging(cuda, dtype, prec, q):
     want = np.matmul(b.astype(np.float64).reshape(nq, m).T, A3).reshape(-1)
     tol = 1e-5 if prec == _lib.PREC_BF16X3 else (2e-6 if dtype == np.float32 else 1e-13)
     assert relerr(c.numpy(), want) <= tol
+
+
+UNALIGNED_COLUMN_CASES = [
+    # (na, pia, q, m): strided rows not on 16-byte boundaries (the column kernel's cp.async ring)
+    ([99, 3001, 7], [1, 2, 3], 2, 5),     # 693 rows: the l range split over the warps of a block
+    ([99, 3001, 7], [1, 2, 3], 2, 16),
+    ([301, 20, 600], [1, 2, 3], 2, 3),    # 180600 rows: one row per lane, no split
+    ([3, 513, 37], [2, 1, 3], 3, 9),      # inner 1539 over two modes, n_q not a multiple of 8
+]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("case", UNALIGNED_COLUMN_CASES)
+def test_unaligned_column_kernel(cuda, oracle_c, case, dtype):
+    """Rows of i that are not 16-byte aligned take the column kernel whose threads stream their
+    rows through a shared-memory ring of asynchronous copies; exact FMA against the C oracle."""
+    import torch
+    na, pia, q, m = case
+    rng = np.random.default_rng(7)
+    nq = na[q - 1]
+    nc = list(na)
+    nc[q - 1] = m
+    wa, wc = ka.dense_strides(na, pia), ka.dense_strides(nc, pia)
+    a = rng.standard_normal(int(np.prod(na))).astype(dtype)
+    b = rng.standard_normal(m * nq).astype(dtype)
+    ta, tb = torch.from_numpy(a).to(cuda), torch.from_numpy(b).to(cuda)
+    tc = torch.full((int(np.prod(nc)),), float("nan"), device=cuda, dtype=ta.dtype)
+    _lib.ttm_raw(_lib.F32 if dtype == np.float32 else _lib.F64, _lib.PREC_DEFAULT, q, len(na), ta.data_ptr(), na, wa,
+                 pia, tb.data_ptr(), [m, nq], [1, 2], tc.data_ptr(), nc, wc, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert _lib.last_kernel() == "colvec", _lib.last_kernel()
+    ref = np.zeros(int(np.prod(nc)), dtype=dtype)
+    oracle_c.ttm(q, a, na, wa, pia, b, [m, nq], [1, 2], ref, nc, wc)
+    assert relerr(tc.cpu().numpy(), ref) <= (1e-13 if dtype == np.float64 else 2e-6)
