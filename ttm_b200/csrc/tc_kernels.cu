@@ -1703,6 +1703,11 @@ bool stream_split(const View3& v, size_t es, int NP, int LB, int sms, StreamShap
     // (96 registers) with 48 KB rings. More bytes in flight per SM than that slowed the
     // write-heavy short-n_q cases; three CTAs of 72 registers lost to both.
     sh.per_sm = (sh.rows || sh.mb > 8 || sh.tiles < (int64_t)sms) ? 1 : 2;
+    if (sh.per_sm == 2) {
+        // one CTA per SM where its last round is much fuller (whole tiles over the slots)
+        auto eff = [&](int64_t slots) { return (double)sh.tiles / (double)(slots * ((sh.tiles + slots - 1) / slots)); };
+        if (eff(sms) >= eff(2 * (int64_t)sms) + 0.08) sh.per_sm = 1;
+    }
     const size_t budget = (sh.per_sm == 2 ? 112 : 227) * 1024 - 1024 - 256;
     const size_t row = (size_t)sh.lb * sh.mb * es;   // staged B bytes per l chunk
     // ring per CTA from hi down to lo while B fits beside it, otherwise fb with B staged a part
