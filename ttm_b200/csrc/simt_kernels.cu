@@ -446,9 +446,9 @@ __global__ void __launch_bounds__(256) colvec_kernel(View3 v)
 
 // colvec_async: the column kernel for rows without 16-byte alignment (one row per lane). Each
 // thread streams its own row's elements A[k][l][i] into a ring of shared memory with 4- or 8-byte
-// asynchronous copies (cp.async, any 4-byte alignment), kColAsyncStages - 1 stages of kColAsyncL
-// l ahead of the one it multiplies, so that many loads are in flight without holding them in
-// registers. A thread reads back only what it copied itself: the ring needs no block barrier,
+// asynchronous copies (cp.async, any 4-byte alignment), kColAsyncStages - 1 stages of LC l
+// (8 float, 4 double) ahead of the one it multiplies, so that many loads are in flight without
+// holding them in registers. A thread reads back only what it copied itself: the ring needs no block barrier,
 // only the thread's own wait on its copy groups. B is staged per chunk of LB l as in colvec.
 constexpr int kColAsyncStages = 4;
 constexpr bool kColAsync = true;   // rows without 16-byte alignment take colvec_async
