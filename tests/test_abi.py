@@ -89,3 +89,17 @@ def test_precision_setting_roundtrip():
     finally:
         _lib.set_precision(old)
     assert _lib.lib().tlibttm_set_precision(42) == -1
+
+
+def test_batched_plan_options_are_checked():
+    """tlibttm_plan_batched_ex rejects a null plan pointer and unknown option bits before any
+    device work."""
+    L = _lib.lib()
+    L.tlibttm_plan_batched_ex.restype = C.c_int
+    L.tlibttm_plan_batched_ex.argtypes = [C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_uint, C.c_void_p]
+    h = C.c_void_p(1)
+    assert L.tlibttm_plan_batched_ex(_lib.F32, _lib.PREC_DEFAULT, 0, None, 0, None) == _lib.ERR_ARG
+    assert "plan pointer is null" in L.tlibttm_last_error().decode()
+    assert L.tlibttm_plan_batched_ex(_lib.F32, _lib.PREC_DEFAULT, 0, None, 2, C.byref(h)) == _lib.ERR_ARG
+    assert "unknown flags" in L.tlibttm_last_error().decode()
+    assert not h.value                      # the plan pointer is cleared on error

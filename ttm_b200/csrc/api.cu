@@ -952,10 +952,10 @@ int tlibttm_plan_batched_ex(int dtype, int precision, size_t count, const tlibtt
                             unsigned flags, tlibttm_plan** plan)
 {
     if (!plan) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_batched: plan pointer is null.");
+    *plan = nullptr;
     if (flags & ~TLIBTTM_PLAN_FEW_LAUNCHES) return fail(TLIBTTM_ERR_ARG, "tlibttm_plan_batched_ex: unknown flags.");
     // small-m problems of at least this many elements of A get launches of their own
     const int64_t small_single_min = (flags & TLIBTTM_PLAN_FEW_LAUNCHES) ? INT64_MAX : kPlanSmallSingleMinElems;
-    *plan = nullptr;
     if (dtype != TLIBTTM_F32 && dtype != TLIBTTM_F64) return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown dtype.");
     if (precision < TLIBTTM_PREC_DEFAULT || precision > TLIBTTM_PREC_AUTO)
         return fail(TLIBTTM_ERR_ARG, "tlibttm: unknown precision.");
